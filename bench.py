@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the FWI2D wave-propagation hot path on B200.
+
+Workload (one "step"): forward modeling of the whole plain-modeling survey -
+151 x 501 cells at 10 m padded by a 100-cell absorbing boundary (351 x 701),
+11 shots, 251 receivers, Ricker 30 Hz, dt 1 ms, nt 3001 (+119 delay samples) -
+through libfwi2d's C ABI.  Metric: FD grid-point updates per second
+(padded points x time steps x shots), whole job over all ranks.
+
+  value     device-resident: model already in HBM, seismograms written to a
+            device buffer; L2 flushed between timed steps (256 MiB write).
+  e2e       fwi_set_model from pinned host memory + fwi_model_survey into a
+            pinned host buffer, both inside the timed region.
+  roofline  the forward-step kernel: 16 algorithmic bytes per grid-point
+            update (read v, Q^t, Q^{t-1}; write Q^{t+1}) x points per launch,
+            over the average launch time in the timed region.
+  cpu_baseline  the oracle's float restatement of compute_pressure +
+            compute_seismogram (OpenMP over all host cores) on one shot.
+
+--impl reference runs the reference's own CUDA build (oracle/_ref/modeling.exe,
+compiled from the reference sources for sm_100a) on the same survey and reports
+updates / its own "Run time"; without that build it times the CPU port.
+
+Multi-GPU (torchrun): every rank models its own copy of the survey (shots are
+independent; no data-path collective) -> weak scaling; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_FALLBACK_GBS = 6650.0
+BYTES_PER_UPDATE = 16
+WORKLOAD = ("plain modeling survey: 151x501 @10 m + 100-cell ABC (351x701), 11 shots, 251 receivers, "
+            "30 Hz Ricker, dt 1 ms, nt 3001")
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def traffic_from_profiles():
+    """DRAM bytes per forward-step launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "fwd_step_config0.txt"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            t = [x.strip() for x in line.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                smax = float(t[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, t[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def make_case():
+    from fwi2d_b200 import synth
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_bench_"))
+    case, vp = synth.config0(d, seed=0)
+    return case, vp
+
+
+def updates_per_step(ctx):
+    d = ctx.dims
+    return d.nsrc * d.nzz * d.nxx * (d.nt + d.tlag)
+
+
+def cpu_baseline(case, vp):
+    """Oracle float restatement of the reference's stencil loop, one shot, all host cores."""
+    from oracle import oracle as O
+    nb = 100
+    wav, tlag = O.wavelet(case.nt, case.dt, case.fmax)
+    vel = O.expand(vp, nb)
+    tab = O.b1d(nb, 0.004)
+    rx = O.indices(case.rx, case.dh, nb)
+    rz = O.indices(case.rz, case.dh, nb)
+    sx = O.indices(case.sx[5:6], case.dh, nb)[0]
+    sz = O.indices(case.sz[5:6], case.dh, nb)[0]
+    t0 = time.perf_counter()
+    O.forward(vel, nb, tab, wav, case.nt, tlag, case.dt, case.dh, (sx, sz), rx, rz, bits=32)
+    t = time.perf_counter() - t0
+    ups = vel.size * (case.nt + tlag)
+    return {"value": ups / t, "unit": "grid-pt updates/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 of 11 shots (shot 6), full {case.nt + tlag} steps on 351x701, float fields with the "
+                      f"reference's double stencil sums, OpenMP over columns; {t:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    case, vp = make_case()
+    exe = ROOT / "oracle" / "_ref" / "modeling.exe"
+    ups = 11 * 351 * 701 * (3001 + 119)
+    line = {"metric": "FD grid-pt updates/s", "unit": "grid-pt updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model)",
+            "config": {"workload": WORKLOAD}}
+    if rank != 0:
+        return None
+    if exe.exists():
+        times = []
+        for k in range(args.warmup + args.steps):
+            r = subprocess.run([str(exe), str(case.params)], capture_output=True, text=True, cwd=str(case.root),
+                               env=dict(os.environ, TERM=os.environ.get("TERM", "dumb")), timeout=900)
+            if r.returncode != 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"reference modeling.exe failed: rc={r.returncode}"}))
+                return None
+            m = re.search(r"Run time:\s*([0-9.eE+-]+)", r.stdout)
+            if k >= args.warmup:
+                times.append(float(m.group(1)))
+        t = max(times)
+        value = ups / (sum(times) / len(times))
+        line.update(value=value, ms_per_step=1e3 * sum(times) / len(times),
+                    cpu_baseline={"value": value, "unit": "grid-pt updates/s", "cores": os.cpu_count(),
+                                  "kind": "reference",
+                                  "sample": "the reference's own CUDA build (oracle/_ref/modeling.exe: reference "
+                                            "sources, FFTW via cuFFTW, sm_100a) on the full 11-shot survey, its "
+                                            "'Run time' (shot loop incl. per-shot file writes); runs on the B200"},
+                    e2e={"value": value, "unit": "grid-pt updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                    reference_build="oracle/_ref/modeling.exe", slowest_step_s=t)
+    else:
+        cb = cpu_baseline(case, vp)
+        line.update(value=cb["value"], ms_per_step=None, cpu_baseline=dict(cb, kind="port"),
+                    e2e={"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    return line
+
+
+def profile_case():
+    """An L2-exceeding forward survey for ncu captures: the FWI survey's grid
+    (301x1701 + 100-cell ABC = 501x1901) with all 81 shots, nt 40 (277 steps)."""
+    from fwi2d_b200 import api, synth
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_prof_"))
+    case, _ = synth.config2(d, seed=2, nt=40)
+    with api.Context(case.params, api.MODE_MODELING) as ctx:
+        ctx.model_survey_raw()
+    print("profile case done")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="for ncu: forward survey of 81 shots on 501x1901 (fields ~630 MB > L2), short time axis")
+    args = ap.parse_args()
+    if args.profile:
+        return profile_case()
+    rank, world, local = dist_env()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from fwi2d_b200 import api
+    case, vp = make_case()
+    ctx = api.Context(case.params, api.MODE_MODELING)
+    d = ctx.dims
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ups = updates_per_step(ctx)
+    nseis = d.nsrc * d.nrec * d.nt
+    d_seis = torch.empty(nseis, dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    for _ in range(args.warmup):
+        ctx.model_survey_dev(d_seis.data_ptr())
+    barrier()
+    times = []
+    launches0 = ctx.launches()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.model_survey_dev(d_seis.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = ctx.launches() - launches0
+    barrier()
+    ms = float(np.mean(times))
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * ups / (ms * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    h_model = torch.from_numpy(np.ascontiguousarray(vp.T).ravel()).pin_memory()
+    h_seis = torch.empty(nseis, dtype=torch.float32).pin_memory()
+    fptr = lambda t: api.C.cast(t.data_ptr(), api._F)
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx._check(ctx._lib.fwi_set_model(ctx._h, fptr(h_model)))
+        ctx._check(ctx._lib.fwi_model_survey(ctx._h, fptr(h_seis)))
+        e1.record(stream)
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = float(np.mean(e2e_times))
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    peak, peak_kind = peaks()
+    n_steps = d.nt + d.tlag
+    bytes_per_launch = BYTES_PER_UPDATE * d.nsrc * d.nzz * d.nxx
+    per_launch_ms = ms / n_steps
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    traffic = traffic_from_profiles()
+    line = {
+        "metric": "FD grid-pt updates/s", "value": value, "unit": "grid-pt updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 4-layer + anomaly model, config 0)",
+        "config": {"workload": WORKLOAD, "shots_per_rank": d.nsrc, "grid": [d.nzz, d.nxx], "time_steps": n_steps,
+                   "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"shot replicas x{world}"},
+        "e2e": {"value": world * ups / (e2e_ms * 1e-3), "unit": "grid-pt updates/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(h_model.numel() * 4), "d2h_bytes_per_step": int(nseis * 4)},
+        "roofline": {"bound": "hbm", "kernel": "fwd_step_kernel<ABC>", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "note": "achieved = 16 B x points per launch / (timed-region time / launches); the 11-shot "
+                             "working set (~23 MB) stays in the 126 MB L2"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(case, vp)
+    ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

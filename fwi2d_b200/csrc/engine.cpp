@@ -1,0 +1,737 @@
+// engine.cpp — see engine.hpp.  Host code compiled with -ffp-contract=off.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <numeric>
+
+namespace fwi {
+
+namespace {
+constexpr int kBufFields = 4;
+// Distinct random boundaries per gradient pass: the RBC seed of pass e is
+// seed + e * kEpochStride (odd constant, so passes never collide).
+constexpr uint64_t kEpochStride = 0xD1B54A32D192ED03ull;
+}  // namespace
+
+void Engine::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(FWI_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+void Engine::sync(const char* what) {
+    check(cudaGetLastError(), what);
+    check(cudaStreamSynchronize(st_), what);
+}
+
+template <typename T>
+static T* dalloc(size_t n, const char* what) {
+    T* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(FWI_ERR_NOMEM, std::string("cudaMalloc of ") + what + " (" + std::to_string(n * sizeof(T)) +
+                                       " bytes): " + cudaGetErrorString(e));
+    }
+    return p;
+}
+
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ------------------------------------------------------------------ set-up
+Engine::Engine(const std::string& params_path, int mode) : P_(params_path), mode_(mode) {
+    if (mode < FWI_MODE_MODELING || mode > FWI_MODE_INVERSION) throw Error(FWI_ERR_ARG, "unknown mode");
+    // set_main_parameters, modeling.cu:17-30
+    nx_ = P_.i("x_samples");
+    nz_ = P_.i("z_samples");
+    dh_ = P_.f("model_spacing");
+    nt_ = P_.i("time_samples");
+    dt_ = P_.f("time_spacing");
+    fmax_ = P_.f("max_frequency");
+    if (nx_ <= 8 || nz_ <= 8) throw Error(FWI_ERR_PARAM, "x_samples and z_samples must exceed 8");
+    if (!(dh_ > 0) || !(dt_ > 0) || !(fmax_ > 0) || nt_ < 2)
+        throw Error(FWI_ERR_PARAM, "model_spacing, time_spacing, max_frequency must be positive, time_samples >= 2");
+    idh2_ = 1.0f / (dh_ * dh_);
+    seed_ = P_.u64_or("rbc_seed", 0);
+    use_graphs_ = std::getenv("FWI2D_NO_GRAPHS") == nullptr;
+
+    wavelet_ = make_wavelet(nt_, dt_, fmax_, &tlag_);
+    geo_ = read_geometry(P_.str("SPS"), P_.str("RPS"));
+    nsrc_ = geo_.nsrc();
+    nrec_ = geo_.nrec();
+
+    check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+
+    if (mode_ == FWI_MODE_MODELING || mode_ == FWI_MODE_INVERSION) {
+        float abc_length = P_.f("abc_length");
+        float abc_factor = P_.f("abc_factor");
+        int nb = boundary_cells(abc_length, dh_);
+        if (nb < 1) throw Error(FWI_ERR_PARAM, "abc_length gives no boundary cells");
+        b1d_ = make_b1d(nb, abc_factor);
+        setup_grid(&abc_, &abc_t_, nb);
+        has_abc_ = true;
+    }
+    if (mode_ == FWI_MODE_MIGRATION || mode_ == FWI_MODE_INVERSION) {
+        const std::string pre = mode_ == FWI_MODE_MIGRATION ? "mig_" : "inv_";
+        rbc_ratio_ = P_.f(pre + "rbc_ratio");
+        rbc_varVp_ = P_.f(pre + "rbc_varVp");
+        float rbc_length = P_.f(pre + "rbc_length");
+        if (!(rbc_ratio_ > 0)) throw Error(FWI_ERR_PARAM, pre + "rbc_ratio must be positive");
+        setup_grid(&rbc_, &rbc_t_, boundary_cells(rbc_length, dh_));
+        has_rbc_ = true;
+    }
+    if (mode_ == FWI_MODE_INVERSION) {
+        zmask_ = P_.f("depth_mask");
+        max_iteration_ = P_.i("max_iteration");
+    }
+
+    alloc_buffers();
+
+    std::vector<float> vp((size_t)nx_ * nz_);
+    read_floats(P_.str("model_file"), vp.data(), vp.size());
+    set_model(vp.data());
+}
+
+void Engine::setup_grid(Grid* g, Tables* t, int nb) {
+    g->nb = nb;
+    g->nxx = nx_ + 2 * nb;
+    g->nzz = nz_ + 2 * nb;
+    g->ldz = round_up(g->nzz, 32);
+    const int nxx = g->nxx;
+    // initialization, modeling.cu:252-277
+    t->src_x.resize(nsrc_);
+    t->src_z.resize(nsrc_);
+    t->rec_x.resize(nrec_);
+    t->rec_z.resize(nrec_);
+    for (int s = 0; s < nsrc_; ++s) {
+        t->src_x[s] = grid_index(geo_.xsrc[s], dh_, nb);
+        t->src_z[s] = grid_index(geo_.zsrc[s], dh_, nb);
+        if (t->src_x[s] < 0 || t->src_x[s] >= nxx || t->src_z[s] < 0 || t->src_z[s] >= g->nzz)
+            throw Error(FWI_ERR_PARAM, "source " + std::to_string(s + 1) + " lies outside the model");
+    }
+    for (int r = 0; r < nrec_; ++r) {
+        t->rec_x[r] = grid_index(geo_.xrec[r], dh_, nb);
+        t->rec_z[r] = grid_index(geo_.zrec[r], dh_, nb);
+        if (t->rec_x[r] < 0 || t->rec_x[r] >= nxx || t->rec_z[r] < 0 || t->rec_z[r] >= g->nzz)
+            throw Error(FWI_ERR_PARAM, "receiver " + std::to_string(r + 1) + " lies outside the model");
+    }
+    t->shots.resize(nsrc_);
+    std::vector<int> rec_pt((size_t)nsrc_ * nrec_);
+    std::vector<int> src_colptr((size_t)nsrc_ * (nxx + 1)), rec_colptr((size_t)nsrc_ * (nxx + 1));
+    std::vector<int> src_z(nsrc_), rec_z((size_t)nsrc_ * nrec_);
+    std::vector<long long> src_soff(nsrc_, 0), rec_soff((size_t)nsrc_ * nrec_);
+    // receivers sorted by column (stable in receiver order)
+    std::vector<int> order(nrec_);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return t->rec_x[a] < t->rec_x[b]; });
+    for (int s = 0; s < nsrc_; ++s) {
+        ShotDesc& d = t->shots[s];
+        d.nxx = nxx;
+        d.nrec = nrec_;
+        d.rec_off = s * nrec_;
+        d.col_off = s * (nxx + 1);
+        d.seis_off = (long long)s * nrec_ * nt_;
+        for (int r = 0; r < nrec_; ++r) rec_pt[(size_t)s * nrec_ + r] = t->rec_z[r] + t->rec_x[r] * g->ldz;
+        // source: one entry per shot
+        src_z[s] = t->src_z[s];
+        for (int j = 0; j <= nxx; ++j) src_colptr[(size_t)s * (nxx + 1) + j] = s + (j > t->src_x[s] ? 1 : 0);
+        // receivers: entries s*nrec .. in column order, amplitudes from the shot's traces
+        int k = s * nrec_;
+        int pos = 0;
+        for (int j = 0; j <= nxx; ++j) {
+            while (pos < nrec_ && t->rec_x[order[pos]] < j) ++pos;
+            rec_colptr[(size_t)s * (nxx + 1) + j] = s * nrec_ + pos;
+        }
+        for (int p = 0; p < nrec_; ++p, ++k) {
+            int r = order[p];
+            rec_z[k] = t->rec_z[r];
+            rec_soff[k] = d.seis_off + (long long)r * nt_;
+        }
+    }
+    auto up = [&](auto* dst, const auto& v, const char* what) {
+        check(cudaMemcpy(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice), what);
+    };
+    t->d_rec_pt = dalloc<int>(rec_pt.size(), "receiver points");
+    up(t->d_rec_pt, rec_pt, "upload receiver points");
+    t->d_src_colptr = dalloc<int>(src_colptr.size(), "source columns");
+    up(t->d_src_colptr, src_colptr, "upload source columns");
+    t->d_src_z = dalloc<int>(src_z.size(), "source rows");
+    up(t->d_src_z, src_z, "upload source rows");
+    t->d_src_soff = dalloc<long long>(src_soff.size(), "source offsets");
+    up(t->d_src_soff, src_soff, "upload source offsets");
+    t->d_rec_colptr = dalloc<int>(rec_colptr.size(), "receiver columns");
+    up(t->d_rec_colptr, rec_colptr, "upload receiver columns");
+    t->d_rec_z = dalloc<int>(rec_z.size(), "receiver rows");
+    up(t->d_rec_z, rec_z, "upload receiver rows");
+    t->d_rec_soff = dalloc<long long>(rec_soff.size(), "receiver offsets");
+    up(t->d_rec_soff, rec_soff, "upload receiver offsets");
+}
+
+void Engine::free_tables(Tables* t) {
+    cudaFree(t->d_rec_pt);
+    cudaFree(t->d_src_colptr);
+    cudaFree(t->d_src_z);
+    cudaFree(t->d_src_soff);
+    cudaFree(t->d_rec_colptr);
+    cudaFree(t->d_rec_z);
+    cudaFree(t->d_rec_soff);
+}
+
+void Engine::alloc_buffers() {
+    const size_t npts = (size_t)nx_ * nz_;
+    const size_t nseis = (size_t)nsrc_ * nrec_ * nt_;
+    fstride_max_ = std::max(has_abc_ ? abc_.fstride() : 0LL, has_rbc_ ? rbc_.fstride() : 0LL);
+    const int nfields = (mode_ == FWI_MODE_MODELING) ? 2 : 7;
+
+    d_vp_ = dalloc<float>(npts, "velocity");
+    d_tmp_ = dalloc<float>(npts, "scratch model");
+    d_wavelet_ = dalloc<float>(nt_, "wavelet");
+    check(cudaMemcpy(d_wavelet_, wavelet_.data(), nt_ * sizeof(float), cudaMemcpyHostToDevice), "upload wavelet");
+    if (has_abc_) {
+        d_b1d_ = dalloc<float>(b1d_.size(), "b1d");
+        check(cudaMemcpy(d_b1d_, b1d_.data(), b1d_.size() * sizeof(float), cudaMemcpyHostToDevice), "upload b1d");
+        d_vel_abc_ = dalloc<float>(abc_.fstride(), "ABC velocity");
+    }
+    if (has_rbc_) d_vel_rbc_base_ = dalloc<float>(rbc_.fstride(), "RBC base velocity");
+    d_seis_ = dalloc<float>(nseis, "seismograms");
+    if (mode_ != FWI_MODE_MODELING) d_data_ = dalloc<float>(nseis, "input data");
+    if (mode_ == FWI_MODE_INVERSION) {
+        d_res_ = dalloc<float>(nseis, "residuals");
+        d_m_ = dalloc<float>(npts, "slowness^2");
+        d_grad_ = dalloc<float>(npts, "gradient");
+    }
+    if (mode_ != FWI_MODE_MODELING) {
+        d_img_ = dalloc<float>(npts, "image / raw gradient");
+        d_illum_ = dalloc<float>(npts, "illumination");
+        check(cudaMemset(d_img_, 0, npts * sizeof(float)), "memset image");
+        check(cudaMemset(d_illum_, 0, npts * sizeof(float)), "memset illumination");
+    }
+    d_partial_ = dalloc<double>((size_t)residual_blocks((size_t)nrec_ * nt_ * std::max(1, nsrc_)) + 1, "partials");
+    d_sum_ = dalloc<double>(1, "sum");
+    d_flag_ = dalloc<int>(1, "flag");
+    d_gmax_ = dalloc<unsigned int>(1, "gmax");
+
+    // shots per batch: the key batch_shots, else what fits in half the free memory
+    size_t free_b = 0, total_b = 0;
+    check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t per_shot = (size_t)nfields * (size_t)fstride_max_ * sizeof(float);
+    size_t fit = per_shot ? (free_b / 2) / per_shot : (size_t)nsrc_;
+    int want = P_.i_or("batch_shots", 0);
+    batch_ = want > 0 ? want : (int)std::min<size_t>((size_t)nsrc_, std::max<size_t>(1, fit));
+    batch_ = std::max(1, std::min(batch_, nsrc_));
+    const size_t fsz = (size_t)batch_ * fstride_max_;
+    const int nbuf = (mode_ == FWI_MODE_MODELING) ? 2 : kBufFields;
+    for (int k = 0; k < nbuf; ++k) fld_[k] = dalloc<float>(fsz, "wavefield");
+    if (mode_ != FWI_MODE_MODELING) {
+        acc_[0] = dalloc<float>(fsz, "accumulator");
+        acc_[1] = dalloc<float>(fsz, "illumination accumulator");
+        d_vel_batch_ = dalloc<float>(fsz, "RBC velocity");
+    }
+    d_batch_ = dalloc<ShotDesc>(batch_, "batch descriptors");
+    d_batch_nxx_ = dalloc<int>(nsrc_, "shot widths");
+    d_batch_id_ = dalloc<int>(nsrc_, "shot ids");
+    d_batch_c0_ = dalloc<int>(nsrc_, "window starts");
+    d_batch_w_ = dalloc<int>(nsrc_, "window widths");
+    d_bump_ptr_ = dalloc<int>(batch_ + 1, "bump offsets");
+    std::vector<int> ids(nsrc_), c0(nsrc_, 0), w(nsrc_, nx_), nxx(nsrc_, has_rbc_ ? rbc_.nxx : abc_.nxx);
+    std::iota(ids.begin(), ids.end(), 0);
+    check(cudaMemcpy(d_batch_id_, ids.data(), nsrc_ * sizeof(int), cudaMemcpyHostToDevice), "upload ids");
+    check(cudaMemcpy(d_batch_c0_, c0.data(), nsrc_ * sizeof(int), cudaMemcpyHostToDevice), "upload c0");
+    check(cudaMemcpy(d_batch_w_, w.data(), nsrc_ * sizeof(int), cudaMemcpyHostToDevice), "upload w");
+    check(cudaMemcpy(d_batch_nxx_, nxx.data(), nsrc_ * sizeof(int), cudaMemcpyHostToDevice), "upload nxx");
+}
+
+Engine::~Engine() {
+    if (st_) cudaStreamSynchronize(st_);
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    if (has_abc_) free_tables(&abc_t_);
+    if (has_rbc_) free_tables(&rbc_t_);
+    void* ptrs[] = {d_vp_, d_m_, d_vel_abc_, d_vel_rbc_base_, d_wavelet_, d_b1d_, d_batch_, d_batch_nxx_,
+                    d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
+                    fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
+                    d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (st_) cudaStreamDestroy(st_);
+}
+
+fwi_dims Engine::dims() const {
+    fwi_dims d;
+    std::memset(&d, 0, sizeof(d));
+    const Grid& g = has_abc_ ? abc_ : rbc_;
+    d.nx = nx_;
+    d.nz = nz_;
+    d.nt = nt_;
+    d.nsrc = nsrc_;
+    d.nrec = nrec_;
+    d.nb = g.nb;
+    d.nxx = g.nxx;
+    d.nzz = g.nzz;
+    d.ldz = g.ldz;
+    d.tlag = tlag_;
+    d.abc_nb = has_abc_ ? abc_.nb : 0;
+    d.rbc_nb = has_rbc_ ? rbc_.nb : 0;
+    d.dh = dh_;
+    d.dt = dt_;
+    d.fmax = fmax_;
+    d.vmin = vmin_;
+    d.vmax = vmax_;
+    return d;
+}
+
+// -------------------------------------------------------------------- model
+void Engine::set_model(const float* vp) {
+    const size_t n = (size_t)nx_ * nz_;
+    float lo = 1e30f, hi = -1e30f;
+    for (size_t k = 0; k < n; ++k) {
+        if (!std::isfinite(vp[k]) || !(vp[k] > 0))
+            throw Error(FWI_ERR_PARAM, "velocity model holds a non-positive or non-finite value at " + std::to_string(k));
+        lo = std::min(lo, vp[k]);
+        hi = std::max(hi, vp[k]);
+    }
+    const double vtop = (double)hi + (has_rbc_ ? std::max(0.0f, rbc_varVp_) : 0.0f);
+    if (vtop * dt_ / dh_ > kCflLimit)
+        throw Error(FWI_ERR_CFL, "unstable: (vmax" + std::string(has_rbc_ ? " + rbc_varVp" : "") + ")*dt/dh = " +
+                                     std::to_string(vtop * dt_ / dh_) + " exceeds " + std::to_string(kCflLimit));
+    vmin_ = lo;
+    vmax_ = hi;
+    check(cudaMemcpyAsync(d_vp_, vp, n * sizeof(float), cudaMemcpyHostToDevice, st_), "upload model");
+    if (d_m_) {
+        launch_slowness2(d_vp_, d_m_, n, st_);
+        ++launches_;
+    }
+    vel_abc_valid_ = vel_rbc_valid_ = false;
+    have_grad_ = false;
+    sync("set_model");
+}
+
+void Engine::get_model(float* vp) {
+    check(cudaMemcpyAsync(vp, d_vp_, (size_t)nx_ * nz_ * sizeof(float), cudaMemcpyDeviceToHost, st_), "get_model");
+    sync("get_model");
+}
+
+void Engine::get_wavelet(float* w) const { std::memcpy(w, wavelet_.data(), wavelet_.size() * sizeof(float)); }
+
+void Engine::get_indices(int shot, int* src_xz, int* rec_x, int* rec_z) const {
+    if (shot < 0 || shot >= nsrc_) throw Error(FWI_ERR_ARG, "shot index out of range");
+    const Tables& t = has_abc_ ? abc_t_ : rbc_t_;
+    if (src_xz) {
+        src_xz[0] = t.src_x[shot];
+        src_xz[1] = t.src_z[shot];
+    }
+    if (rec_x) std::copy(t.rec_x.begin(), t.rec_x.end(), rec_x);
+    if (rec_z) std::copy(t.rec_z.begin(), t.rec_z.end(), rec_z);
+}
+
+void Engine::expand_to(const Grid& g, const float* d_model, float* d_out) {
+    launch_expand(d_model, nz_, nx_, d_out, 0, d_batch_c0_, d_batch_w_, 1, g.nb, g.nzz, g.ldz, g.nxx, st_);
+    ++launches_;
+}
+
+void Engine::ensure_rbc_base() {
+    if (!vel_rbc_valid_) {
+        expand_to(rbc_, d_vp_, d_vel_rbc_base_);
+        vel_rbc_valid_ = true;
+    }
+}
+
+// ------------------------------------------------------------------ batches
+void Engine::upload_batch(const Tables& t, int s0, int ns) {
+    check(cudaMemcpyAsync(d_batch_, t.shots.data() + s0, ns * sizeof(ShotDesc), cudaMemcpyHostToDevice, st_),
+          "upload batch");
+    // the pageable source is staged before the call returns; the stream orders
+    // the copy before the graph that reads it
+}
+
+void Engine::build_rbc(int s0, int ns) {
+    const uint64_t seed_eff = seed_ + (uint64_t)rbc_epoch_ * kEpochStride;
+    std::vector<std::vector<Bump>> per(ns);
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < ns; ++k)
+        per[k] = make_bumps(rbc_.nxx, rbc_.nzz, rbc_.nb, dh_, rbc_ratio_, rbc_varVp_, seed_eff, (uint32_t)(s0 + k));
+    std::vector<int> ptr(ns + 1, 0);
+    for (int k = 0; k < ns; ++k) ptr[k + 1] = ptr[k] + (int)per[k].size();
+    std::vector<BumpDev> all((size_t)std::max(1, ptr[ns]));
+    for (int k = 0; k < ns; ++k)
+        for (size_t p = 0; p < per[k].size(); ++p) {
+            const Bump& b = per[k][p];
+            all[ptr[k] + p] = BumpDev{b.xc, b.zc, b.r, b.A, b.factor};
+        }
+    if (all.size() > bumps_cap_) {
+        check(cudaStreamSynchronize(st_), "sync before bump realloc");
+        cudaFree(d_bumps_);
+        bumps_cap_ = all.size() * 2;
+        d_bumps_ = dalloc<BumpDev>(bumps_cap_, "bumps");
+    }
+    check(cudaMemcpyAsync(d_bumps_, all.data(), all.size() * sizeof(BumpDev), cudaMemcpyHostToDevice, st_),
+          "upload bumps");
+    check(cudaMemcpyAsync(d_bump_ptr_, ptr.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, st_),
+          "upload bump offsets");
+    RbcArgs a;
+    a.base = d_vel_rbc_base_;
+    a.base_stride = 0;
+    a.out = d_vel_batch_;
+    a.out_stride = rbc_.fstride();
+    a.nxx = d_batch_nxx_ + s0;
+    a.shot_id = d_batch_id_ + s0;
+    a.bumps = d_bumps_;
+    a.bump_ptr = d_bump_ptr_;
+    a.nzz = rbc_.nzz;
+    a.ldz = rbc_.ldz;
+    a.nb = rbc_.nb;
+    a.max_nxx = rbc_.nxx;
+    a.dh = dh_;
+    a.varVp = rbc_varVp_;
+    a.vmin = vmin_;
+    a.vmax = vmax_;
+    a.seed = seed_eff;
+    launch_rbc(a, ns, st_);
+    ++launches_;
+    // bump vectors are pageable: synchronous staging makes them safe to drop
+    check(cudaGetLastError(), "rbc launch");
+}
+
+void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride, bool abc,
+                         bool record, float* d_seis) {
+    const long long fs = g.fstride();
+    float* F0 = fld_[0];
+    float* F1 = fld_[1];
+    check(cudaMemsetAsync(F0, 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
+    check(cudaMemsetAsync(F1, 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
+    InjTable inj{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, 0, idh2_};
+    launch_inject_points(F0, fs, d_batch_, ns, inj, g.ldz, st_);
+    ++launches_;
+    const int N = nt_ + tlag_;
+    const dim3 grid = step_grid(g.ldz, g.nxx, ns);
+    const float dt2idh2 = dt_ * dt_ * idh2_;
+    auto body = [&]() {
+        for (int tt = 0; tt < N; ++tt) {
+            FwdArgs a;
+            a.shots = d_batch_;
+            a.vel = vel;
+            a.vel_stride = vel_stride;
+            a.cur = (tt % 2 == 0) ? F0 : F1;
+            a.nxt = (tt % 2 == 0) ? F1 : F0;
+            a.fstride = fs;
+            a.ldz = g.ldz;
+            a.nzz = g.nzz;
+            a.nb = g.nb;
+            a.dt2idh2 = dt2idh2;
+            a.b1d = abc ? d_b1d_ : nullptr;
+            a.inj = inj;
+            a.inj.sample = (tt + 1 < nt_) ? tt + 1 : -1;
+            a.rec_pt = t.d_rec_pt;
+            a.seis = d_seis;
+            a.rec_sample = (record && tt > tlag_) ? tt - tlag_ : -1;
+            a.nt = nt_;
+            launch_fwd_step(a, grid, st_);
+        }
+    };
+    const long long key = (((long long)(record ? kFwdRecord : kFwdNoRecord) * 2 + (abc ? 0 : 1)) * 4 +
+                           (&g == &abc_ ? 0 : 1)) * 1000000LL + ns;
+    if (use_graphs_) {
+        auto it = graphs_.find(key);
+        if (it == graphs_.end()) {
+            cudaGraph_t graph;
+            check(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "begin capture");
+            body();
+            check(cudaStreamEndCapture(st_, &graph), "end capture");
+            cudaGraphExec_t exec;
+            check(cudaGraphInstantiate(&exec, graph, 0), "instantiate graph");
+            cudaGraphDestroy(graph);
+            it = graphs_.emplace(key, exec).first;
+        }
+        check(cudaGraphLaunch(it->second, st_), "graph launch");
+    } else {
+        body();
+    }
+    launches_ += N;
+    check(cudaGetLastError(), "forward propagation");
+}
+
+void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride,
+                          bool gradient, const float* d_series) {
+    const long long fs = g.fstride();
+    const int N = nt_ + tlag_;
+    float* X = fld_[N % 2];        // Q^N      (Ps of migration.cu:76)
+    float* Y = fld_[(N + 1) % 2];  // Q^{N-1}  (Psold)
+    float* R0 = fld_[2];
+    float* R1 = fld_[3];
+    const size_t bytes = (size_t)ns * fs * sizeof(float);
+    check(cudaMemsetAsync(R0, 0, bytes, st_), "memset Pr");
+    check(cudaMemsetAsync(R1, 0, bytes, st_), "memset Prold");
+    check(cudaMemsetAsync(acc_[0], 0, bytes, st_), "memset accumulator");
+    check(cudaMemsetAsync(acc_[1], 0, bytes, st_), "memset accumulator");
+    InjTable inj{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, d_series, nt_ - 1, idh2_};
+    launch_inject_points(R0, fs, d_batch_, ns, inj, g.ldz, st_);
+    ++launches_;
+    const dim3 grid = step_grid(g.ldz, g.nxx, ns);
+    const float dt2idh2 = dt_ * dt_ * idh2_;
+    auto body = [&]() {
+        for (int b = 0; b < N; ++b) {
+            BwdArgs a;
+            a.shots = d_batch_;
+            a.vel = vel;
+            a.vel_stride = vel_stride;
+            a.ps_st = (b % 2 == 0) ? Y : X;
+            a.ps_io = (b % 2 == 0) ? X : Y;
+            a.pr_st = (b % 2 == 0) ? R0 : R1;
+            a.pr_io = (b % 2 == 0) ? R1 : R0;
+            a.fstride = fs;
+            a.acc_a = acc_[0];
+            a.acc_b = acc_[1];
+            a.acc_stride = fs;
+            a.ldz = g.ldz;
+            a.nzz = g.nzz;
+            a.dt2idh2 = dt2idh2;
+            a.dt = dt_;
+            a.idh2 = idh2_;
+            a.inj = inj;
+            a.inj.sample = (b + 1 < nt_) ? nt_ - 1 - (b + 1) : -1;
+            launch_bwd_step(a, gradient, grid, st_);
+        }
+    };
+    const long long key = ((long long)(gradient ? kBwdGradient : kBwdImage) * 8 + 4 + (&g == &abc_ ? 0 : 1)) *
+                              1000000LL + ns;
+    if (use_graphs_) {
+        auto it = graphs_.find(key);
+        if (it == graphs_.end()) {
+            cudaGraph_t graph;
+            check(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "begin capture");
+            body();
+            check(cudaStreamEndCapture(st_, &graph), "end capture");
+            cudaGraphExec_t exec;
+            check(cudaGraphInstantiate(&exec, graph, 0), "instantiate graph");
+            cudaGraphDestroy(graph);
+            it = graphs_.emplace(key, exec).first;
+        }
+        check(cudaGraphLaunch(it->second, st_), "graph launch");
+    } else {
+        body();
+    }
+    launches_ += N;
+    check(cudaGetLastError(), "backward propagation");
+}
+
+void Engine::check_finite(const float* d, size_t n, const char* what) {
+    check(cudaMemsetAsync(d_flag_, 0, sizeof(int), st_), "memset flag");
+    launch_check_finite(d, n, d_flag_, st_);
+    ++launches_;
+    int flag = 0;
+    check(cudaMemcpyAsync(&flag, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, st_), "read flag");
+    sync(what);
+    if (flag) throw Error(FWI_ERR_NAN, std::string(what) + ": non-finite values (unstable propagation?)");
+}
+
+// ---------------------------------------------------------------- modeling
+void Engine::model_shots(int s0, int ns, float* out, bool out_on_device) {
+    if (!has_abc_) throw Error(FWI_ERR_STATE, "modeling needs a context created for modeling or inversion");
+    if (s0 < 0 || ns < 1 || s0 + ns > nsrc_) throw Error(FWI_ERR_ARG, "shot range out of bounds");
+    if (!vel_abc_valid_) {
+        expand_to(abc_, d_vp_, d_vel_abc_);
+        vel_abc_valid_ = true;
+    }
+    const size_t per = (size_t)nrec_ * nt_;
+    check(cudaMemsetAsync(d_seis_ + (size_t)s0 * per, 0, (size_t)ns * per * sizeof(float), st_), "memset seis");
+    for (int b0 = s0; b0 < s0 + ns; b0 += batch_) {
+        const int nb = std::min(batch_, s0 + ns - b0);
+        upload_batch(abc_t_, b0, nb);
+        run_forward(abc_, abc_t_, nb, d_vel_abc_, 0, true, true, d_seis_);
+    }
+    check_finite(d_seis_ + (size_t)s0 * per, (size_t)ns * per, "modeling");
+    if (out) {
+        check(cudaMemcpyAsync(out, d_seis_ + (size_t)s0 * per, (size_t)ns * per * sizeof(float),
+                              out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st_),
+              "copy seismograms");
+    }
+    sync("model_shots");
+}
+
+// --------------------------------------------------------------- migration
+void Engine::rtm_reset() {
+    if (!has_rbc_) throw Error(FWI_ERR_STATE, "migration needs a context created for migration or inversion");
+    const size_t n = (size_t)nx_ * nz_;
+    check(cudaMemsetAsync(d_img_, 0, n * sizeof(float), st_), "memset image");
+    check(cudaMemsetAsync(d_illum_, 0, n * sizeof(float), st_), "memset illumination");
+    sync("rtm_reset");
+}
+
+void Engine::rtm_shots(int s0, int ns, const float* data, bool data_on_device) {
+    if (!has_rbc_) throw Error(FWI_ERR_STATE, "migration needs a context created for migration or inversion");
+    if (s0 < 0 || ns < 1 || s0 + ns > nsrc_) throw Error(FWI_ERR_ARG, "shot range out of bounds");
+    const size_t per = (size_t)nrec_ * nt_;
+    if (data)
+        check(cudaMemcpyAsync(d_data_ + (size_t)s0 * per, data, (size_t)ns * per * sizeof(float),
+                              data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_),
+              "upload migration data");
+    ensure_rbc_base();
+    for (int b0 = s0; b0 < s0 + ns; b0 += batch_) {
+        const int nb = std::min(batch_, s0 + ns - b0);
+        upload_batch(rbc_t_, b0, nb);
+        build_rbc(b0, nb);
+        run_forward(rbc_, rbc_t_, nb, d_vel_batch_, rbc_.fstride(), false, false, d_seis_);
+        run_backward(rbc_, rbc_t_, nb, d_vel_batch_, rbc_.fstride(), false, d_data_);
+        launch_crop_sum(acc_[0], rbc_.fstride(), nb, rbc_.nb, rbc_.ldz, nz_, nx_, d_img_, true, st_);
+        launch_crop_sum(acc_[1], rbc_.fstride(), nb, rbc_.nb, rbc_.ldz, nz_, nx_, d_illum_, true, st_);
+        launches_ += 2;
+    }
+    check_finite(d_img_, (size_t)nx_ * nz_, "migration");
+}
+
+void Engine::rtm_image(float* image) {
+    if (!has_rbc_) throw Error(FWI_ERR_STATE, "no migration state");
+    launch_rtm_post(d_img_, d_illum_, nz_, nx_, idh2_, d_tmp_, st_);
+    ++launches_;
+    check(cudaMemcpyAsync(image, d_tmp_, (size_t)nx_ * nz_ * sizeof(float), cudaMemcpyDeviceToHost, st_),
+          "copy image");
+    sync("rtm_image");
+}
+
+void Engine::rtm_raw(float* img, float* illum) {
+    if (!has_rbc_) throw Error(FWI_ERR_STATE, "no migration state");
+    const size_t n = (size_t)nx_ * nz_ * sizeof(float);
+    if (img) check(cudaMemcpyAsync(img, d_img_, n, cudaMemcpyDeviceToHost, st_), "copy image");
+    if (illum) check(cudaMemcpyAsync(illum, d_illum_, n, cudaMemcpyDeviceToHost, st_), "copy illumination");
+    sync("rtm_raw");
+}
+
+void Engine::random_boundary(int shot, float* out) {
+    if (!has_rbc_) throw Error(FWI_ERR_STATE, "no random-boundary grid in this context");
+    if (shot < 0 || shot >= nsrc_) throw Error(FWI_ERR_ARG, "shot index out of range");
+    ensure_rbc_base();
+    build_rbc(shot, 1);
+    std::vector<float> pitched((size_t)rbc_.fstride());
+    check(cudaMemcpyAsync(pitched.data(), d_vel_batch_, pitched.size() * sizeof(float), cudaMemcpyDeviceToHost, st_),
+          "copy random boundary");
+    sync("random_boundary");
+    for (int j = 0; j < rbc_.nxx; ++j)
+        std::memcpy(out + (size_t)j * rbc_.nzz, pitched.data() + (size_t)j * rbc_.ldz, rbc_.nzz * sizeof(float));
+}
+
+// ---------------------------------------------------------------- inversion
+void Engine::set_observed(const float* obs, bool on_device) {
+    if (mode_ != FWI_MODE_INVERSION) throw Error(FWI_ERR_STATE, "observed data needs an inversion context");
+    const size_t n = (size_t)nsrc_ * nrec_ * nt_;
+    check(cudaMemcpyAsync(d_data_, obs, n * sizeof(float),
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_),
+          "upload observed data");
+    sync("set_observed");
+    have_obs_ = true;
+}
+
+double Engine::residual_of(int s0, int ns, const float* d_obs, const float* d_cal, float* d_res) {
+    const size_t per = (size_t)nrec_ * nt_;
+    const size_t off = (size_t)s0 * per, n = (size_t)ns * per;
+    launch_residual(d_obs + off, d_cal + off, d_res + off, n, d_partial_, d_sum_, st_);
+    launches_ += 2;
+    double h = 0.0;
+    check(cudaMemcpyAsync(&h, d_sum_, sizeof(double), cudaMemcpyDeviceToHost, st_), "read misfit");
+    sync("residual");
+    return h;
+}
+
+double Engine::compute_gradient(bool with_gradient) {
+    if (mode_ != FWI_MODE_INVERSION) throw Error(FWI_ERR_STATE, "gradient needs an inversion context");
+    if (!have_obs_) throw Error(FWI_ERR_STATE, "observed data not set");
+    const size_t npts = (size_t)nx_ * nz_;
+    if (!vel_abc_valid_) {
+        expand_to(abc_, d_vp_, d_vel_abc_);
+        vel_abc_valid_ = true;
+    }
+    if (with_gradient) {
+        ensure_rbc_base();
+        check(cudaMemsetAsync(d_img_, 0, npts * sizeof(float), st_), "memset gradient");
+        check(cudaMemsetAsync(d_illum_, 0, npts * sizeof(float), st_), "memset illumination");
+    }
+    const size_t per = (size_t)nrec_ * nt_;
+    double sum = 0.0;
+    for (int b0 = 0; b0 < nsrc_; b0 += batch_) {
+        const int nb = std::min(batch_, nsrc_ - b0);
+        check(cudaMemsetAsync(d_seis_ + (size_t)b0 * per, 0, (size_t)nb * per * sizeof(float), st_), "memset seis");
+        upload_batch(abc_t_, b0, nb);
+        run_forward(abc_, abc_t_, nb, d_vel_abc_, 0, true, true, d_seis_);
+        sum += residual_of(b0, nb, d_data_, d_seis_, d_res_);
+        if (with_gradient) {
+            upload_batch(rbc_t_, b0, nb);
+            build_rbc(b0, nb);
+            run_forward(rbc_, rbc_t_, nb, d_vel_batch_, rbc_.fstride(), false, false, d_seis_);
+            run_backward(rbc_, rbc_t_, nb, d_vel_batch_, rbc_.fstride(), true, d_res_);
+            launch_crop_sum(acc_[0], rbc_.fstride(), nb, rbc_.nb, rbc_.ldz, nz_, nx_, d_img_, true, st_);
+            launch_crop_sum(acc_[1], rbc_.fstride(), nb, rbc_.nb, rbc_.ldz, nz_, nx_, d_illum_, true, st_);
+            launches_ += 2;
+        }
+    }
+    if (with_gradient) {
+        launch_grad_post(d_img_, d_illum_, nz_, nx_, idh2_, (int)(zmask_ / dh_), d_grad_, d_gmax_, st_);
+        launch_scale_by_inverse(d_grad_, npts, d_gmax_, st_);
+        launches_ += 2;
+        ++rbc_epoch_;
+        have_grad_ = true;
+    }
+    sync("compute_gradient");
+    return sum;
+}
+
+void Engine::get_gradient(float* g) {
+    if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
+    check(cudaMemcpyAsync(g, d_grad_, (size_t)nx_ * nz_ * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy gradient");
+    sync("get_gradient");
+}
+
+void Engine::get_gradient_raw(float* g, float* illum) {
+    if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
+    const size_t n = (size_t)nx_ * nz_ * sizeof(float);
+    if (g) check(cudaMemcpyAsync(g, d_img_, n, cudaMemcpyDeviceToHost, st_), "copy raw gradient");
+    if (illum) check(cudaMemcpyAsync(illum, d_illum_, n, cudaMemcpyDeviceToHost, st_), "copy illumination");
+    sync("get_gradient_raw");
+}
+
+double Engine::linesearch_trial(float alpha) {
+    if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
+    const size_t npts = (size_t)nx_ * nz_;
+    launch_trial_velocity(d_m_, d_grad_, alpha, d_tmp_, npts, st_);
+    ++launches_;
+    expand_to(abc_, d_tmp_, d_vel_abc_);
+    vel_abc_valid_ = false;  // holds the trial model now
+    const size_t per = (size_t)nrec_ * nt_;
+    double sum = 0.0;
+    for (int b0 = 0; b0 < nsrc_; b0 += batch_) {
+        const int nb = std::min(batch_, nsrc_ - b0);
+        check(cudaMemsetAsync(d_seis_ + (size_t)b0 * per, 0, (size_t)nb * per * sizeof(float), st_), "memset seis");
+        upload_batch(abc_t_, b0, nb);
+        run_forward(abc_, abc_t_, nb, d_vel_abc_, 0, true, true, d_seis_);
+        sum += residual_of(b0, nb, d_data_, d_seis_, d_res_);
+    }
+    return sum;
+}
+
+float Engine::optimization(float f0) {
+    // inversion.cu:286-308, in float as there
+    float dm = (1.0f / (vmin_ * vmin_)) - (1.0f / (vmax_ * vmax_));
+    float a0 = 0.00f * dm;
+    float a1 = 0.02f * dm;
+    float a2 = 0.05f * dm;
+    float f1 = sqrtf((float)linesearch_trial(a1));
+    float f2 = sqrtf((float)linesearch_trial(a2));
+    float num = (a1 * a1 - a2 * a2) * f0 + (a2 * a2 - a0 * a0) * f1 + (a0 * a0 - a1 * a1) * f2;
+    float den = (a1 - a2) * f0 + (a2 - a0) * f1 + (a0 - a1) * f2;
+    return 0.5f * (num / den);
+}
+
+void Engine::update_model(float step, float* vp_out) {
+    if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
+    const size_t npts = (size_t)nx_ * nz_;
+    launch_update_model(d_m_, d_grad_, step, d_vp_, npts, st_);
+    ++launches_;
+    vel_abc_valid_ = vel_rbc_valid_ = false;
+    if (vp_out) check(cudaMemcpyAsync(vp_out, d_vp_, npts * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy model");
+    sync("update_model");
+}
+
+}  // namespace fwi

@@ -1,0 +1,166 @@
+// engine.hpp — device state and workflows behind the C ABI (fwi2d.h).
+//
+// One Engine per context.  It owns one CUDA stream, the survey-sized device
+// buffers (seismograms, data, residuals), the per-batch wavefields and the
+// CUDA graphs of the time loops.  Shots are processed in batches: every step
+// of a batch is one launch over all of its shots (blockIdx.z = shot), and the
+// whole nt+tlag step loop is captured once per (propagation kind, batch size)
+// as a CUDA graph and replayed for every batch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/fwi2d.h"
+#include "host.hpp"
+#include "kargs.h"
+#include "kernels.h"
+
+namespace fwi {
+
+class Engine {
+public:
+    Engine(const std::string& params_path, int mode);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    fwi_dims dims() const;
+    cudaStream_t stream() const { return st_; }
+    void set_seed(uint64_t s) { seed_ = s; }
+    long long launches(bool reset) { long long c = launches_; if (reset) launches_ = 0; return c; }
+
+    void set_model(const float* vp_host);          // nz x nx
+    void get_model(float* vp_host);
+    void get_wavelet(float* w) const;
+    void get_indices(int shot, int* src_xz, int* rec_x, int* rec_z) const;
+
+    // modeling
+    void model_shots(int s0, int ns, float* seis_out, bool out_on_device);
+    // migration
+    void rtm_reset();
+    void rtm_shots(int s0, int ns, const float* data, bool data_on_device);
+    void rtm_image(float* image_host);
+    void rtm_raw(float* img_host, float* illum_host);
+    // inversion
+    void set_observed(const float* obs, bool on_device);
+    double compute_gradient(bool with_gradient);
+    void get_gradient(float* g_host);
+    void get_gradient_raw(float* g_host, float* illum_host);
+    double linesearch_trial(float alpha);
+    float optimization(float f0);
+    void update_model(float step, float* vp_out);
+    // random boundary of one shot on the RBC grid, nzz x nxx unpitched
+    void random_boundary(int shot, float* out_host);
+
+    // accessors used by the executables
+    const ParamFile& params() const { return P_; }
+    const Geometry& geometry() const { return geo_; }
+    int nx() const { return nx_; }
+    int nz() const { return nz_; }
+    int nt() const { return nt_; }
+    float dh() const { return dh_; }
+    float dt() const { return dt_; }
+    float fmax() const { return fmax_; }
+    int max_iteration() const { return max_iteration_; }
+
+private:
+    struct Grid {
+        int nb = 0, nxx = 0, nzz = 0, ldz = 0;
+        long long fstride() const { return (long long)ldz * nxx; }
+    };
+    // Per-grid shot tables (indices depend on nb).
+    struct Tables {
+        std::vector<ShotDesc> shots;       // one per survey shot
+        std::vector<int> src_x, src_z;     // grid indices
+        std::vector<int> rec_x, rec_z;     // per receiver (same for all shots)
+        int* d_rec_pt = nullptr;           // nsrc*nrec
+        int* d_src_colptr = nullptr;       // nsrc*(nxx+1)
+        int* d_src_z = nullptr;
+        long long* d_src_soff = nullptr;
+        int* d_rec_colptr = nullptr;       // nsrc*(nxx+1)
+        int* d_rec_z = nullptr;            // nsrc*nrec, sorted by column
+        long long* d_rec_soff = nullptr;
+    };
+    enum Kind { kFwdRecord = 0, kFwdNoRecord = 1, kBwdImage = 2, kBwdGradient = 3 };
+
+    void setup_grid(Grid* g, Tables* t, int nb);
+    void free_tables(Tables* t);
+    void alloc_buffers();
+    void upload_batch(const Tables& t, int s0, int ns);
+    void expand_to(const Grid& g, const float* d_model_interior, float* d_out);
+    void build_rbc(int s0, int ns);
+    // forward propagation of the current batch (fields end in fld_[0..1])
+    void run_forward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride, bool abc,
+                     bool record, float* d_seis);
+    void run_backward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride,
+                      bool gradient, const float* d_series);
+    void check(cudaError_t e, const char* what);
+    void sync(const char* what);
+    void check_finite(const float* d, size_t n, const char* what);
+    void ensure_rbc_base();
+    double residual_of(int s0, int ns, const float* d_obs, const float* d_cal, float* d_res);
+
+    ParamFile P_;
+    int mode_;
+    Geometry geo_;
+    int nx_ = 0, nz_ = 0, nt_ = 0, tlag_ = 0, nsrc_ = 0, nrec_ = 0;
+    float dh_ = 0, dt_ = 0, fmax_ = 0, idh2_ = 0;
+    float vmin_ = 0, vmax_ = 0;
+    std::vector<float> wavelet_, b1d_;
+    Grid abc_, rbc_;
+    Tables abc_t_, rbc_t_;
+    bool has_abc_ = false, has_rbc_ = false;
+    float rbc_ratio_ = 0, rbc_varVp_ = 0;
+    float zmask_ = 0;
+    int max_iteration_ = 0;
+    uint64_t seed_ = 0;
+    long long rbc_epoch_ = 0;
+    int batch_ = 1;
+    long long launches_ = 0;
+
+    cudaStream_t st_ = nullptr;
+    // model state
+    float* d_vp_ = nullptr;          // interior velocity nz x nx
+    float* d_m_ = nullptr;           // slowness^2 (inversion)
+    float* d_vel_abc_ = nullptr;     // padded ABC-grid velocity (shared by shots)
+    float* d_vel_rbc_base_ = nullptr;// padded RBC-grid edge-replicated velocity
+    bool vel_abc_valid_ = false, vel_rbc_valid_ = false;
+    float* d_wavelet_ = nullptr;
+    float* d_b1d_ = nullptr;
+    // batch state
+    ShotDesc* d_batch_ = nullptr;    // device copy of the batch's shot descriptors
+    ShotDesc* h_batch_ = nullptr;    // pinned staging
+    int* d_batch_nxx_ = nullptr;     // per batch shot: width (RBC kernel)
+    int* d_batch_id_ = nullptr;      // per batch shot: survey index
+    int* d_batch_c0_ = nullptr;      // per batch shot: window start column
+    int* d_batch_w_ = nullptr;       // per batch shot: window width
+    int* d_bump_ptr_ = nullptr;
+    BumpDev* d_bumps_ = nullptr;
+    size_t bumps_cap_ = 0;
+    float* fld_[4] = {nullptr, nullptr, nullptr, nullptr};
+    float* acc_[2] = {nullptr, nullptr};
+    float* d_vel_batch_ = nullptr;   // per-shot RBC velocity
+    long long fstride_max_ = 0;
+    // survey buffers
+    float* d_seis_ = nullptr;        // modeled / calculated data, nsrc*nrec*nt
+    float* d_data_ = nullptr;        // observed (inversion) or input (migration) data
+    float* d_res_ = nullptr;         // residual / adjoint source
+    double* d_partial_ = nullptr;
+    double* d_sum_ = nullptr;
+    int* d_flag_ = nullptr;
+    unsigned int* d_gmax_ = nullptr;
+    // cropped accumulators nz x nx
+    float* d_img_ = nullptr;
+    float* d_illum_ = nullptr;
+    float* d_grad_ = nullptr;        // post-processed gradient
+    float* d_tmp_ = nullptr;
+    bool have_obs_ = false, have_grad_ = false;
+    // time-loop graphs, key = (kind, grid, batch size)
+    std::map<long long, cudaGraphExec_t> graphs_;
+    bool use_graphs_ = true;
+};
+
+}  // namespace fwi

@@ -1,0 +1,77 @@
+// kargs.h — argument blocks of the propagation kernels (host and device).
+//
+// Device layout of every padded grid: column-major with z fastest like the
+// reference (idx = i + j*nzz, src/modeling/modeling.cu:308-309), but with the
+// column pitch ldz rounded up to a multiple of 32 floats so that every column
+// starts on a 128-byte boundary and float4 / TMA accesses stay aligned.  Rows
+// nzz..ldz-1 hold zeros.  A batch of shots stores its fields back to back
+// with a fixed per-shot stride (fstride = ldz * max columns).
+#pragma once
+#include <stdint.h>
+
+namespace fwi {
+
+// Finite-difference coefficients of the reference (modeling.cuh:9-13):
+// 1/560, 8/315, 1/5, 8/5, 205/72, as the decimal literals given there.
+constexpr double kFDM1 = 0.001785714285;
+constexpr double kFDM2 = 0.025396825396;
+constexpr double kFDM3 = 0.200000000000;
+constexpr double kFDM4 = 1.600000000000;
+constexpr double kFDM5 = 2.847222222222;
+
+struct ShotDesc {
+    int nxx;             // padded width (columns) of this shot's grid
+    int nrec;            // receivers of this shot
+    int rec_off;         // first entry of the shot in rec_pt[]
+    int col_off;         // first entry of the shot's injection column table
+    long long seis_off;  // float offset of the shot's nt x nrec trace-major block
+};
+
+// Point injections into the field written by a step (the source of a forward
+// propagation, the receivers of an adjoint / migration back-propagation).
+// Points of column j of shot s are entries colptr[col_off+j] ..
+// colptr[col_off+j+1]-1; each adds scale * series[soff + sample].
+struct InjTable {
+    const int* colptr;
+    const int* z;
+    const long long* soff;
+    const float* series;
+    int sample;          // sample index of this step, or -1 for no injection
+    float scale;
+};
+
+struct FwdArgs {
+    const ShotDesc* shots;    // batch-local shot descriptors
+    const float* vel;         // velocity, padded layout
+    long long vel_stride;     // per-shot stride of vel (0: shared by all shots)
+    const float* cur;         // Q^t (read, stencil)
+    float* nxt;               // Q^{t-1} on entry, Q^{t+1} on exit (pointwise)
+    long long fstride;        // per-shot stride of cur / nxt
+    int ldz, nzz, nb;
+    float dt2idh2;            // dt^2 / dh^2
+    const float* b1d;         // ABC damping profile (nb floats), NULL for none
+    InjTable inj;
+    const int* rec_pt;        // receiver points z + x*ldz, per shot at rec_off
+    float* seis;              // trace-major seismograms
+    int rec_sample;           // sample recorded at this step, or -1
+    int nt;
+};
+
+struct BwdArgs {
+    const ShotDesc* shots;
+    const float* vel;
+    long long vel_stride;
+    const float* ps_st;       // source field read by the stencil (Psold)
+    float* ps_io;             // source field read pointwise and overwritten (Ps)
+    const float* pr_st;       // receiver field read by the stencil (Pr)
+    float* pr_io;             // receiver field read pointwise and overwritten (Prold)
+    long long fstride;
+    float* acc_a;             // image (RTM) or gradient (FWI), per shot
+    float* acc_b;             // source illumination, per shot
+    long long acc_stride;
+    int ldz, nzz;
+    float dt2idh2, dt, idh2;
+    InjTable inj;             // receiver-side injection into pr_io
+};
+
+}  // namespace fwi

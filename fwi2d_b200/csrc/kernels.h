@@ -1,0 +1,65 @@
+// kernels.h — launch wrappers of the device kernels (all enqueue on `st`).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kargs.h"
+
+namespace fwi {
+
+// ---- k_stencil.cu ------------------------------------------------------------
+dim3 step_grid(int ldz, int max_nxx, int nshots);
+void launch_fwd_step(const FwdArgs& a, dim3 grid, cudaStream_t st);
+void launch_bwd_step(const BwdArgs& a, bool gradient, dim3 grid, cudaStream_t st);
+
+// ---- k_rbc.cu ----------------------------------------------------------------
+struct BumpDev { float xc, zc, r, A, factor; };
+struct RbcArgs {
+    const float* base;         // edge-replicated velocity, padded layout
+    long long base_stride;     // per-shot stride of base (0: shared)
+    float* out;                // random-boundary velocity per shot
+    long long out_stride;
+    const int* nxx;            // per-shot padded width
+    const int* shot_id;        // survey index of each shot (RNG stream)
+    const BumpDev* bumps;
+    const int* bump_ptr;       // per shot: bumps[bump_ptr[s] .. bump_ptr[s+1])
+    int nzz, ldz, nb, max_nxx;
+    float dh, varVp, vmin, vmax;
+    uint64_t seed;
+};
+void launch_rbc(const RbcArgs& a, int nshots, cudaStream_t st);
+
+// ---- k_util.cu ---------------------------------------------------------------
+// padded(i,j) = model(clamp(i-nb), c0 + clamp(j-nb, 0, w-1)), nz x nx model,
+// one window per shot (c0[s], w[s]); rows nzz..ldz-1 are zeroed.
+void launch_expand(const float* model, int nz, int nx, float* out, long long out_stride, const int* c0,
+                   const int* w, int nshots, int nb, int nzz, int ldz, int max_nxx, cudaStream_t st);
+// out(i,j) = sum over shots of padded(i+nb, j+nb); nz x nx.
+void launch_crop_sum(const float* padded, long long stride, int nshots, int nb, int ldz, int nz, int nx,
+                     float* out, bool accumulate, cudaStream_t st);
+// RTM post-processing (migration.cu:90-115): q = img/illum, out = -d2q/dz2 * idh2.
+void launch_rtm_post(const float* img, const float* illum, int nz, int nx, float idh2, float* out, cudaStream_t st);
+// Gradient post-processing (inversion.cu:136-165) without the final scaling:
+// q = g/illum, out = -d2q/dz2 * idh2 below row zmask_i, |out| max into *gmax_bits.
+void launch_grad_post(const float* g, const float* illum, int nz, int nx, float idh2, int zmask_i, float* out,
+                      unsigned int* gmax_bits, cudaStream_t st);
+void launch_scale_by_inverse(float* x, size_t n, const unsigned int* gmax_bits, cudaStream_t st);
+// res = obs - cal over n samples, per-block FP64 partial sums of res^2 into
+// partial[], then a fixed-order sum into *out.  Deterministic.
+int  residual_blocks(size_t n);
+void launch_residual(const float* obs, const float* cal, float* res, size_t n, double* partial, double* out,
+                     cudaStream_t st);
+// vp = 1/sqrtf(m - alpha*g)  (inversion.cu:312-317)
+void launch_trial_velocity(const float* m, const float* g, float alpha, float* vp, size_t n, cudaStream_t st);
+// m -= step*g; vp = 1/sqrtf(m)  (inversion.cu:346-352)
+void launch_update_model(float* m, const float* g, float step, float* vp, size_t n, cudaStream_t st);
+// m = 1/(vp*vp)  (inversion.cu:101-109)
+void launch_slowness2(const float* vp, float* m, size_t n, cudaStream_t st);
+// Sets *flag to 1 when any of x[0..n) is not finite.
+void launch_check_finite(const float* x, size_t n, int* flag, cudaStream_t st);
+// Adds scale*series[soff[k] + sample] at the listed points of each shot
+// (the injection of time level 0, before the first step).
+void launch_inject_points(float* field, long long fstride, const ShotDesc* shots, int nshots, InjTable inj,
+                          int ldz, cudaStream_t st);
+
+}  // namespace fwi

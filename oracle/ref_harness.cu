@@ -1,0 +1,117 @@
+// ref_harness.cu — drives the reference's own CUDA code to produce golden
+// vectors (TEST INFRASTRUCTURE; built by `make -C oracle ref` into oracle/_ref).
+//
+// It links the reference sources where they lie (src/admin, src/geometry,
+// src/modeling, src/migration, src/inversion) and, through a subclass of the
+// reference's Modeling class, runs:
+//   * set_parameters (wavelet through FFTW -> cuFFTW, ABC tables, model, geometry)
+//   * per shot: initialization + forward_solver (compute_pressure +
+//     compute_seismogram), dumping the seismogram and the final two fields;
+//   * optionally the backward loops of Migration::backward_propagation
+//     (inject_seismogram + cross_correlation, migration.cu:61-81) and of
+//     Inversion::backward_propagation (inject_adjoint + build_gradient,
+//     inversion.cu:230-248) on a forward run without ABC, for a given padded
+//     velocity and given input traces.
+// The reference's random-boundary kernels are NOT called: random_boundary_bg
+// and random_boundary_gp index past the end of Vp and X for the threads of the
+// last block (modeling.cu:467-524), so the harness takes the boundary velocity
+// as an input file instead.
+//
+// usage: ref_harness <parameters.txt> <outdir> [vel_padded.bin data_prefix]
+//   without the optional arguments: ABC modeling of every shot;
+//   with them: ABC off, d_Vp replaced by vel_padded.bin (nzz x nxx), then per
+//   shot forward + RTM backward and forward + gradient backward, with the input
+//   traces of shot k read from <data_prefix><k>.bin.
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "inversion/inversion.cuh"
+#include "migration/migration.cuh"
+#include "modeling/modeling.cuh"
+
+static void save(const std::string& path, const float* d_ptr, size_t n) {
+    std::vector<float> h(n);
+    cudaMemcpy(h.data(), d_ptr, n * sizeof(float), cudaMemcpyDeviceToHost);
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) { std::fprintf(stderr, "cannot write %s\n", path.c_str()); std::exit(2); }
+    std::fwrite(h.data(), sizeof(float), n, f);
+    std::fclose(f);
+}
+
+static std::vector<float> load(const std::string& path, size_t n) {
+    std::vector<float> h(n);
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f || std::fread(h.data(), sizeof(float), n, f) != n) { std::fprintf(stderr, "cannot read %s\n", path.c_str()); std::exit(2); }
+    std::fclose(f);
+    return h;
+}
+
+class Driver : public Modeling {
+public:
+    void run(const std::string& params, const std::string& out, const char* vel_file, const char* data_prefix) {
+        parameters = params;
+        set_parameters();
+        save(out + "/wavelet.bin", d_wavelet, nt);
+        save(out + "/b1d.bin", d_b1d, nb);
+        const int nrec = geometry->nrec;
+        if (vel_file) {
+            ABC = false;
+            std::vector<float> v = load(vel_file, (size_t)matsize);
+            cudaMemcpy(d_Vp, v.data(), matsize * sizeof(float), cudaMemcpyHostToDevice);
+        }
+        float *d_Pr = nullptr, *d_Prold = nullptr, *d_acc = nullptr, *d_ill = nullptr;
+        if (vel_file) {
+            cudaMalloc(&d_Pr, matsize * sizeof(float));
+            cudaMalloc(&d_Prold, matsize * sizeof(float));
+            cudaMalloc(&d_acc, matsize * sizeof(float));
+            cudaMalloc(&d_ill, matsize * sizeof(float));
+        }
+        for (srcId = 0; srcId < geometry->nsrc; srcId++) {
+            initialization();
+            cudaMemset(d_seismogram, 0, (size_t)nt * nrec * sizeof(float));
+            forward_solver();
+            const std::string k = std::to_string(srcId + 1);
+            save(out + "/seis_" + k + ".bin", d_seismogram, (size_t)nt * nrec);
+            save(out + "/p_" + k + ".bin", d_P, matsize);
+            save(out + "/pold_" + k + ".bin", d_Pold, matsize);
+            if (!vel_file) continue;
+            std::vector<float> data = load(std::string(data_prefix) + k + ".bin", (size_t)nt * nrec);
+            for (int mode = 0; mode < 2; ++mode) {
+                if (mode == 1) forward_solver();  // fresh source field for the gradient pass
+                cudaMemcpy(d_seismogram, data.data(), data.size() * sizeof(float), cudaMemcpyHostToDevice);
+                cudaMemset(d_Pr, 0, matsize * sizeof(float));
+                cudaMemset(d_Prold, 0, matsize * sizeof(float));
+                cudaMemset(d_acc, 0, matsize * sizeof(float));
+                cudaMemset(d_ill, 0, matsize * sizeof(float));
+                for (int tId = 0; tId < nt + tlag; tId++) {
+                    if (mode == 0) {
+                        inject_seismogram<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
+                        cross_correlation<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, idh2, dt);
+                    } else {
+                        inject_adjoint<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
+                        build_gradient<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, nt, dt, idh2);
+                    }
+                    std::swap(d_P, d_Pold);
+                    std::swap(d_Pr, d_Prold);
+                }
+                const char* tag = mode == 0 ? "image" : "grad";
+                save(out + "/" + tag + "_" + k + ".bin", d_acc, matsize);
+                save(out + "/" + tag + "_illum_" + k + ".bin", d_ill, matsize);
+            }
+        }
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e)); std::exit(3); }
+        std::printf("nb=%d nxx=%d nzz=%d tlag=%d nt=%d nrec=%d\n", nb, nxx, nzz, tlag, nt, nrec);
+    }
+};
+
+int main(int argc, char** argv) {
+    if (argc != 3 && argc != 5) {
+        std::fprintf(stderr, "usage: %s parameters.txt outdir [vel_padded.bin data_prefix]\n", argv[0]);
+        return 1;
+    }
+    Driver d;
+    d.run(argv[1], argv[2], argc == 5 ? argv[3] : nullptr, argc == 5 ? argv[4] : nullptr);
+    return 0;
+}
