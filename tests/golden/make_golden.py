@@ -6,7 +6,10 @@ sources).  Needs a GPU; run from the repository root:
 
 Cases (seeded synthetic inputs, written with fwi2d_b200.synth):
   A  48 x 96 at 10 m, 20-cell ABC, nt 500, 30 Hz, 3 shots, 24 receivers:
-     modeling.exe seismograms + the harness's wavelet, b1d and final fields;
+     the harness's seismograms with the source injected in its own launch
+     (the golden values), its wavelet, b1d and final fields, and - to record the
+     reference's injection race - modeling.exe's and the harness's raw
+     forward_solver seismograms;
   B  case A geometry, ABC off, padded velocity = the oracle's random boundary of
      the smoothed model: forward + migration back-propagation
      (inject_seismogram + cross_correlation) and forward + adjoint
@@ -42,14 +45,24 @@ def run(cmd, cwd):
     return r.stdout
 
 
+def ld(p, n):
+    return np.fromfile(p, np.float32, n)
+
+
 def modeling_case(tmp, tag, **kw):
+    """modeling.exe as shipped, then the harness (raw and race-free injection)."""
     case, vp = synth.small_case(Path(tmp) / tag, **kw)
     run([REF / "modeling.exe", case.params], case.root)
     nt, nr = case.nt, len(case.rx)
     us = int(np.float32(1e6) * np.float32(case.dt))
-    seis = np.stack([np.fromfile(case.root / "data" / f"seismogram_nt{nt}_nr{nr}_{us}us_shot_{s + 1}.bin", np.float32)
-                     .reshape(nr, nt).T for s in range(len(case.sx))])
-    return case, vp, seis
+    exe = np.stack([ld(case.root / "data" / f"seismogram_nt{nt}_nr{nr}_{us}us_shot_{s + 1}.bin", nt * nr)
+                    .reshape(nr, nt).T for s in range(len(case.sx))])
+    h = Path(tmp) / f"h{tag}"
+    h.mkdir()
+    run([REF / "ref_harness", case.params, h], case.root)
+    seis = lambda name: np.stack([ld(h / f"{name}_{s + 1}.bin", nt * nr).reshape(nr, nt).T
+                                  for s in range(len(case.sx))])
+    return case, vp, exe, seis("seis_raw"), seis("seis"), h
 
 
 def main():
@@ -58,24 +71,19 @@ def main():
     with tempfile.TemporaryDirectory() as tmp:
         # ---- A
         kwA = dict(seed=11)
-        caseA, vpA, seisA = modeling_case(tmp, "A", **kwA)
-        hA = Path(tmp) / "hA"
-        hA.mkdir()
-        run([REF / "ref_harness", caseA.params, hA], caseA.root)
+        caseA, vpA, exeA, rawA, seisA, hA = modeling_case(tmp, "A", **kwA)
         nb = 20
         nzz, nxx = caseA.nz + 2 * nb, caseA.nx + 2 * nb
-        ld = lambda p, n: np.fromfile(p, np.float32, n)
         wavelet = ld(hA / "wavelet.bin", caseA.nt)
         b1d = ld(hA / "b1d.bin", nb)
-        seis_h = np.stack([ld(hA / f"seis_{s + 1}.bin", caseA.nt * len(caseA.rx)).reshape(len(caseA.rx), caseA.nt).T
-                           for s in range(len(caseA.sx))])
         p1 = ld(hA / "p_1.bin", nzz * nxx).reshape(nxx, nzz).T
         pold1 = ld(hA / "pold_1.bin", nzz * nxx).reshape(nxx, nzz).T
         # ---- C
         kwC = dict(seed=13, nz=37, nx=71, dh=12.5, nt=400, fmax=25.0, nshots=2, nrec=15, boundary=150.0)
-        caseC, vpC, seisC = modeling_case(tmp, "C", **kwC)
-        np.savez_compressed(OUT / "ref_modeling.npz", A_kwargs=repr(kwA), A_seis=seisA, A_seis_harness=seis_h,
-                            A_wavelet=wavelet, A_b1d=b1d, A_p1=p1, A_pold1=pold1, C_kwargs=repr(kwC), C_seis=seisC)
+        caseC, vpC, exeC, rawC, seisC, _ = modeling_case(tmp, "C", **kwC)
+        np.savez_compressed(OUT / "ref_modeling.npz", A_kwargs=repr(kwA), A_seis=seisA, A_seis_exe=exeA,
+                            A_seis_raw=rawA, A_wavelet=wavelet, A_b1d=b1d, A_p1=p1, A_pold1=pold1,
+                            C_kwargs=repr(kwC), C_seis=seisC, C_seis_exe=exeC)
         # ---- B
         smooth = synth.smooth_model(vpA, caseA.dh, 40.0)
         base = O.expand(smooth, nb)

@@ -68,9 +68,14 @@ def test_golden_modeling_pins_oracle(tag, nb):
 
 
 @needs_mod
-def test_golden_harness_matches_executable():
+def test_golden_records_the_reference_injection_race():
+    """modeling.exe as shipped loses source injections on a B200 (the atomicAdd of
+    thread 0 races with the owner's in-place `P *= damper`, modeling.cu:316-341):
+    its traces are far from the race-free run of the same kernels."""
     g = np.load(MOD)
-    assert rel_l2(g["A_seis_harness"][:, 1:], g["A_seis"][:, 1:]) < 1e-6
+    ref = g["A_seis"]
+    errs = [rel_l2(g["A_seis_exe"][s][1:], ref[s][1:]) for s in range(ref.shape[0])]
+    assert max(errs) > 1e-2, errs
 
 
 @needs_bwd
