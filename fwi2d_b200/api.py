@@ -81,6 +81,7 @@ SIGNATURES = {
     "fwi_util_bumps": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64,
                                  C.c_uint32, _F, C.c_int, _I]),
     "fwi_util_normal": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _F]),
+    "fwi_residual_noalloc": (C.c_int, [_P, _P, _P, C.c_size_t, _P, _P]),
 }
 
 

@@ -35,6 +35,7 @@ CU_SOURCES = {
     "k_stencil.cu": [],
     "k_util.cu": [],
     "k_rbc.cu": ["-fmad=false"],
+    "k_noalloc.cu": [],
 }
 CXX_SOURCES = ["host.cpp", "engine.cpp", "capi.cpp"]
 APPS = ["modeling", "migration", "inversion"]

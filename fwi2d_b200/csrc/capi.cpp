@@ -274,6 +274,14 @@ int fwi_util_normal(uint64_t seed, uint32_t shot, uint32_t stream, uint64_t ctr,
     return FWI_OK;
 }
 
+int fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, size_t n, double* d_sum,
+                         void* stream) {
+    std::string err;
+    int rc = fwi::residual_noalloc(d_obs, d_cal, d_res, n, d_sum, static_cast<cudaStream_t>(stream), &err);
+    if (rc != FWI_OK) g_create_error = err;
+    return rc;
+}
+
 int fwi_launch_count(fwi_ctx* ctx, long long* count, int reset) {
     if (!count) return arg_error(ctx, "NULL count");
     return guarded(ctx, [&](fwi::Engine& e) { *count = e.launches(reset != 0); });

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "kargs.h"
 
 namespace fwi {
@@ -61,5 +63,10 @@ void launch_check_finite(const float* x, size_t n, int* flag, cudaStream_t st);
 // (the injection of time level 0, before the first step).
 void launch_inject_points(float* field, long long fstride, const ShotDesc* shots, int nshots, InjTable inj,
                           int ldz, cudaStream_t st);
+
+// ---- k_noalloc.cu --------------------------------------------------------------
+size_t noalloc_max_samples();
+int residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, size_t n, double* d_sum,
+                     cudaStream_t st, std::string* err);
 
 }  // namespace fwi

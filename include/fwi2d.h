@@ -161,6 +161,22 @@ int  fwi_util_bumps(int nxx, int nzz, int nb, float dh, float ratio, float varVp
 /* Standard-normal draw `ctr` of the random-boundary stream (seed, shot, stream). */
 int  fwi_util_normal(uint64_t seed, uint32_t shot, uint32_t stream, uint64_t ctr, float* out);
 
+/* ---- residual and misfit without device allocation -----------------------
+ * No counterpart in the reference: it has no entry point of this kind.
+ * d_res = d_obs - d_cal over n samples and *d_sum = sum(d_res^2) in FP64, for
+ * callers that cannot call cudaMalloc - an application whose own pool owns
+ * all device memory, code inside a stream capture, or a loop that must not
+ * take cudaMalloc's implicit synchronisation.  All pointers are device memory
+ * (d_sum: one double); `stream` is a cudaStream_t (NULL: default stream) and
+ * the call only enqueues work.  The scratch is a 64 KiB file-scope device
+ * array, so n is limited to FWI_NOALLOC_MAX_SAMPLES (FWI_ERR_ARG beyond it;
+ * split larger inputs).  The first call on a device looks the array up, so
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+#define FWI_NOALLOC_MAX_SAMPLES ((size_t)8192 * 8192)
+int  fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, size_t n, double* d_sum,
+                          void* stream);
+
 /* ---- timing / diagnostics ----------------------------------------------- */
 /* Kernel launches issued by the context since creation (or the last reset). */
 int  fwi_launch_count(fwi_ctx* ctx, long long* count, int reset);
