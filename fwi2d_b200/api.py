@@ -82,6 +82,7 @@ SIGNATURES = {
                                  C.c_uint32, _F, C.c_int, _I]),
     "fwi_util_normal": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _F]),
     "fwi_residual_noalloc": (C.c_int, [_P, _P, _P, C.c_size_t, _P, _P]),
+    "fwi_describe": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
 }
 
 
@@ -164,6 +165,11 @@ class Context:
     def param(self, key: str) -> str:
         buf = C.create_string_buffer(4096)
         self._check(self._lib.fwi_get_param(self._h, key.encode(), buf, 4096))
+        return buf.value.decode()
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(256)
+        self._check(self._lib.fwi_describe(self._h, buf, 256))
         return buf.value.decode()
 
     def launches(self, reset: bool = False) -> int:

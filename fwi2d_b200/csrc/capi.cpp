@@ -282,6 +282,14 @@ int fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, s
     return rc;
 }
 
+int fwi_describe(fwi_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !ctx->eng || !buf || len == 0) return FWI_ERR_ARG;
+    const std::string& s = ctx->eng->last_fwd_plan;
+    if (s.size() + 1 > len) return FWI_ERR_ARG;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return FWI_OK;
+}
+
 int fwi_launch_count(fwi_ctx* ctx, long long* count, int reset) {
     if (!count) return arg_error(ctx, "NULL count");
     return guarded(ctx, [&](fwi::Engine& e) { *count = e.launches(reset != 0); });

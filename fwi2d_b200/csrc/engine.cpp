@@ -1,12 +1,15 @@
 // engine.cpp — see engine.hpp.  Host code compiled with -ffp-contract=off.
 #include "engine.hpp"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <numeric>
+#include <sstream>
 
 namespace fwi {
 
@@ -27,6 +30,14 @@ void Engine::check(cudaError_t e, const char* what) {
 void Engine::sync(const char* what) {
     check(cudaGetLastError(), what);
     check(cudaStreamSynchronize(st_), what);
+    if (d_err_) {
+        int err = 0;
+        check(cudaMemcpy(&err, d_err_, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+        if (err) {
+            cudaMemset(d_err_, 0, sizeof(int));
+            throw Error(FWI_ERR_TIMEOUT, std::string(what) + ": a kernel's bounded wait for its tile loads gave up");
+        }
+    }
 }
 
 template <typename T>
@@ -60,6 +71,8 @@ Engine::Engine(const std::string& params_path, int mode) : P_(params_path), mode
     idh2_ = 1.0f / (dh_ * dh_);
     seed_ = P_.u64_or("rbc_seed", 0);
     use_graphs_ = std::getenv("FWI2D_NO_GRAPHS") == nullptr;
+    fwd_kernel_ = P_.str_or("fwd_kernel", "auto");
+    if (const char* e = std::getenv("FWI2D_FWD_KERNEL")) fwd_kernel_ = e;
 
     wavelet_ = make_wavelet(nt_, dt_, fmax_, &tlag_);
     geo_ = read_geometry(P_.str("SPS"), P_.str("RPS"));
@@ -226,8 +239,13 @@ void Engine::alloc_buffers() {
     batch_ = want > 0 ? want : (int)std::min<size_t>((size_t)nsrc_, std::max<size_t>(1, fit));
     batch_ = std::max(1, std::min(batch_, nsrc_));
     const size_t fsz = (size_t)batch_ * fstride_max_;
-    const int nbuf = (mode_ == FWI_MODE_MODELING) ? 2 : kBufFields;
-    for (int k = 0; k < nbuf; ++k) fld_[k] = dalloc<float>(fsz, "wavefield");
+    for (int k = 0; k < kBufFields; ++k) fld_[k] = dalloc<float>(fsz, "wavefield");
+    d_tile_base_ = dalloc<int>(batch_ + 1, "tile table");
+    d_err_ = dalloc<int>(1, "error flag");
+    check(cudaMemset(d_err_, 0, sizeof(int)), "memset error flag");
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "SM count");
     if (mode_ != FWI_MODE_MODELING) {
         acc_[0] = dalloc<float>(fsz, "accumulator");
         acc_[1] = dalloc<float>(fsz, "illumination accumulator");
@@ -255,7 +273,7 @@ Engine::~Engine() {
     void* ptrs[] = {d_vp_, d_m_, d_vel_abc_, d_vel_rbc_base_, d_wavelet_, d_b1d_, d_batch_, d_batch_nxx_,
                     d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
-                    d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_};
+                    d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (st_) cudaStreamDestroy(st_);
@@ -397,27 +415,269 @@ void Engine::build_rbc(int s0, int ns) {
     check(cudaGetLastError(), "rbc launch");
 }
 
+// ------------------------------------------------------- TMA forward plans
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+            throw Error(FWI_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+}  // namespace
+
+const CUtensorMap& Engine::tmap(const float* base, const Grid& g, int nshots, int boxz, int boxx) {
+    std::ostringstream k;
+    k << (const void*)base << ':' << g.ldz << ':' << g.nxx << ':' << nshots << ':' << g.fstride() << ':' << boxz << ':'
+      << boxx;
+    auto it = tmaps_.find(k.str());
+    if (it != tmaps_.end()) return it->second;
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)g.ldz, (cuuint64_t)g.nxx, (cuuint64_t)nshots};
+    cuuint64_t strides[2] = {(cuuint64_t)g.ldz * 4, (cuuint64_t)g.fstride() * 4};
+    cuuint32_t box[3] = {(cuuint32_t)boxz, (cuuint32_t)boxx, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(FWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return tmaps_.emplace(k.str(), m).first->second;
+}
+
+void Engine::upload_tile_base(const Grid& g, int ns, int tx) {
+    const int ntz = (g.ldz + fwd_tma_rows() - 1) / fwd_tma_rows();
+    std::vector<int> base(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        const int nxx = h_shot_nxx(g, s);
+        base[s + 1] = base[s] + ntz * ((nxx + tx - 1) / tx);
+    }
+    check(cudaMemcpyAsync(d_tile_base_, base.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, st_),
+          "upload tile table");
+}
+
+void Engine::launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, const Tables& t, int ns,
+                                 const float* vel, long long vel_stride, bool abc, float* cur, float* old,
+                                 float* out1, float* out2, int tt, bool record, float* d_seis) {
+    const FwdTmaConfig& c = two ? p.cfg : p.tail;
+    FwdTmaArgs a;
+    a.shots = d_batch_;
+    a.tile_base = d_tile_base_;
+    a.ns = ns;
+    a.ntz = (g.ldz + fwd_tma_rows() - 1) / fwd_tma_rows();
+    a.ldz = g.ldz;
+    a.nzz = g.nzz;
+    a.nb = g.nb;
+    a.fstride = g.fstride();
+    a.vel_shared = vel_stride == 0 ? 1 : 0;
+    a.dt2idh2 = dt_ * dt_ * idh2_;
+    a.b1d = abc ? d_b1d_ : nullptr;
+    a.inj = InjTable{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, -1, idh2_};
+    a.sample1 = (tt + 1 < nt_) ? tt + 1 : -1;
+    a.sample2 = (two && tt + 2 < nt_) ? tt + 2 : -1;
+    a.rec = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, nullptr, -1, 0.0f};
+    a.seis = record ? d_seis : nullptr;
+    a.rec_sample0 = (record && tt > tlag_) ? tt - tlag_ : -1;
+    a.rec_sample1 = (record && two && tt + 1 > tlag_) ? tt + 1 - tlag_ : -1;
+    a.out1 = out1;
+    a.out2 = out2;
+    a.err = d_err_;
+    const CUtensorMap& mc = tmap(cur, g, batch_, fwd_tma_box_cur_z(c), fwd_tma_box_cur_x(c));
+    const CUtensorMap& mo = tmap(old, g, batch_, fwd_tma_box_pt_z(c), fwd_tma_box_pt_x(c));
+    const CUtensorMap& mv = tmap(vel, g, vel_stride ? batch_ : 1, fwd_tma_box_pt_z(c), fwd_tma_box_pt_x(c));
+    check(launch_fwd_tma(c, mc, mo, mv, a, two ? p.grid : p.tail_grid, st_), "forward TMA launch");
+}
+
+double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                                  long long vel_stride, bool abc) {
+    const long long fs = g.fstride();
+    const dim3 grid = step_grid(g.ldz, g.nxx, ns);
+    const int reps = 8;  // launches timed
+    auto one = [&](int k) {
+        if (p.kind == 0) {
+            FwdArgs a;
+            a.shots = d_batch_;
+            a.vel = vel;
+            a.vel_stride = vel_stride;
+            a.cur = fld_[k % 2];
+            a.nxt = fld_[(k + 1) % 2];
+            a.fstride = fs;
+            a.ldz = g.ldz;
+            a.nzz = g.nzz;
+            a.nb = g.nb;
+            a.dt2idh2 = dt_ * dt_ * idh2_;
+            a.b1d = abc ? d_b1d_ : nullptr;
+            a.inj = InjTable{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, -1, idh2_};
+            a.rec_pt = t.d_rec_pt;
+            a.seis = nullptr;
+            a.rec_sample = -1;
+            a.nt = nt_;
+            launch_fwd_step(a, grid, st_);
+        } else {
+            upload_tile_base(g, ns, p.cfg.TX);
+            launch_fwd_tma_step(p, p.cfg.T == 2, g, t, ns, vel, vel_stride, abc, fld_[k % 2], fld_[(k + 1) % 2],
+                                fld_[2 + k % 2], fld_[3 - k % 2], 0, false, nullptr);
+        }
+    };
+    one(0);  // first use: module load, tensor maps
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    check(cudaEventRecord(e0, st_), "event record");
+    for (int k = 0; k < reps; ++k) one(k);
+    check(cudaEventRecord(e1, st_), "event record");
+    check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int steps = reps * (p.kind == 1 ? p.cfg.T : 1);
+    return 1e3 * ms / steps;
+}
+
+Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel,
+                                 long long vel_stride) {
+    const long long key = ((long long)(&g == &abc_ ? 0 : 1) * 2 + (abc ? 1 : 0)) * 4 * 1000000LL +
+                          (vel_stride ? 1000000LL : 0) + ns;
+    auto it = plans_.find(key);
+    if (it != plans_.end()) return it->second;
+    auto make = [&](int T, int TX, int S) {
+        FwdPlan p;
+        p.kind = 1;
+        p.cfg = FwdTmaConfig{T, TX, S};
+        p.tail = FwdTmaConfig{1, TX, TX == 32 ? 2 : 3};
+        int ctas = 0, ctas_t = 0;
+        if (fwd_tma_configure(&ctas, p.cfg) != cudaSuccess || ctas < 1) {
+            cudaGetLastError();
+            p.kind = -1;
+            return p;
+        }
+        if (fwd_tma_configure(&ctas_t, p.tail) != cudaSuccess || ctas_t < 1) {
+            cudaGetLastError();
+            p.kind = -1;
+            return p;
+        }
+        p.grid = sm_count_ * ctas;
+        p.tail_grid = sm_count_ * ctas_t;
+        return p;
+    };
+    std::vector<FwdPlan> cands;
+    if (fwd_kernel_ == "simple") {
+        cands.push_back(FwdPlan{});
+    } else if (fwd_kernel_.rfind("tma:", 0) == 0) {
+        int T = 0, TX = 0, S = 0;
+        if (std::sscanf(fwd_kernel_.c_str() + 4, "%d,%d,%d", &T, &TX, &S) != 3 || !fwd_tma_supported({T, TX, S}))
+            throw Error(FWI_ERR_PARAM, "fwd_kernel '" + fwd_kernel_ + "' is not a compiled TMA variant");
+        cands.push_back(make(T, TX, S));
+    } else if (fwd_kernel_ == "auto" || fwd_kernel_ == "tma") {
+        if (fwd_kernel_ == "auto") cands.push_back(FwdPlan{});
+        const int variants[][3] = {{1, 32, 2}, {1, 32, 3}, {1, 16, 3}, {1, 16, 4}, {2, 32, 2}, {2, 16, 2}, {2, 16, 3}};
+        for (const auto& v : variants) cands.push_back(make(v[0], v[1], v[2]));
+    } else {
+        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma or tma:T,TX,S");
+    }
+    FwdPlan best;
+    double best_us = 1e30;
+    for (auto& c : cands) {
+        if (c.kind < 0) continue;
+        if (cands.size() == 1) {
+            best = c;
+            break;
+        }
+        c.us_per_step = time_fwd_candidate(c, g, t, ns, vel, vel_stride, abc);
+        if (c.us_per_step < best_us) {
+            best_us = c.us_per_step;
+            best = c;
+        }
+    }
+    sync("forward autotune");
+    plans_[key] = best;
+    return best;
+}
+
 void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride, bool abc,
                          bool record, float* d_seis) {
     const long long fs = g.fstride();
-    float* F0 = fld_[0];
-    float* F1 = fld_[1];
-    check(cudaMemsetAsync(F0, 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
-    check(cudaMemsetAsync(F1, 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
+    const FwdPlan plan = fwd_plan(g, t, ns, abc, vel, vel_stride);
+    {
+        std::ostringstream d;
+        if (plan.kind == 0) d << "simple";
+        else d << "tma T=" << plan.cfg.T << " TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
+        last_fwd_plan = d.str();
+    }
+    float* B[4] = {fld_[0], fld_[1], fld_[2], fld_[3]};
+    check(cudaMemsetAsync(B[0], 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
+    check(cudaMemsetAsync(B[1], 0, (size_t)ns * fs * sizeof(float), st_), "memset field");
     InjTable inj{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, 0, idh2_};
-    launch_inject_points(F0, fs, d_batch_, ns, inj, g.ldz, st_);
+    launch_inject_points(B[0], fs, d_batch_, ns, inj, g.ldz, st_);
     ++launches_;
     const int N = nt_ + tlag_;
     const dim3 grid = step_grid(g.ldz, g.nxx, ns);
     const float dt2idh2 = dt_ * dt_ * idh2_;
+    int launches_in_loop = 0;
+    // buffer roles after the loop (indices into B)
+    int cur = 0, old = 1;
+    if (plan.kind == 1) {
+        upload_tile_base(g, ns, plan.cfg.TX);
+        int f0 = 2, f1 = 3, tt = 0;
+        cur = 0;
+        old = 1;
+        while (tt < N) {
+            const bool two = plan.cfg.T == 2 && tt + 1 < N;
+            const int pc = cur, po = old;
+            if (two) {
+                old = f0;
+                cur = f1;
+                f0 = pc;
+                f1 = po;
+                tt += 2;
+            } else {
+                old = pc;
+                cur = f0;
+                f0 = po;
+                tt += 1;
+            }
+            ++launches_in_loop;
+        }
+    } else {
+        cur = N % 2;
+        old = (N + 1) % 2;
+        launches_in_loop = N;
+    }
     auto body = [&]() {
+        if (plan.kind == 1) {
+            int c = 0, o = 1, f0 = 2, f1 = 3, tt = 0;
+            while (tt < N) {
+                const bool two = plan.cfg.T == 2 && tt + 1 < N;
+                launch_fwd_tma_step(plan, two, g, t, ns, vel, vel_stride, abc, B[c], B[o], B[f0], two ? B[f1] : nullptr,
+                                    tt, record, d_seis);
+                const int pc = c, po = o;
+                if (two) {
+                    o = f0;
+                    c = f1;
+                    f0 = pc;
+                    f1 = po;
+                    tt += 2;
+                } else {
+                    o = pc;
+                    c = f0;
+                    f0 = po;
+                    tt += 1;
+                }
+            }
+            return;
+        }
         for (int tt = 0; tt < N; ++tt) {
             FwdArgs a;
             a.shots = d_batch_;
             a.vel = vel;
             a.vel_stride = vel_stride;
-            a.cur = (tt % 2 == 0) ? F0 : F1;
-            a.nxt = (tt % 2 == 0) ? F1 : F0;
+            a.cur = (tt % 2 == 0) ? B[0] : B[1];
+            a.nxt = (tt % 2 == 0) ? B[1] : B[0];
             a.fstride = fs;
             a.ldz = g.ldz;
             a.nzz = g.nzz;
@@ -433,8 +693,10 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
             launch_fwd_step(a, grid, st_);
         }
     };
-    const long long key = (((long long)(record ? kFwdRecord : kFwdNoRecord) * 2 + (abc ? 0 : 1)) * 4 +
-                           (&g == &abc_ ? 0 : 1)) * 1000000LL + ns;
+    fwd_cur_ = B[cur];
+    fwd_old_ = B[old];
+    const long long key = ((((long long)(record ? kFwdRecord : kFwdNoRecord) * 2 + (abc ? 0 : 1)) * 4 +
+                            (&g == &abc_ ? 0 : 1)) * 8 + (vel_stride ? 1 : 0)) * 1000000LL + ns;
     if (use_graphs_) {
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
@@ -451,7 +713,7 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     } else {
         body();
     }
-    launches_ += N;
+    launches_ += launches_in_loop;
     check(cudaGetLastError(), "forward propagation");
 }
 
@@ -459,10 +721,14 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
                           bool gradient, const float* d_series) {
     const long long fs = g.fstride();
     const int N = nt_ + tlag_;
-    float* X = fld_[N % 2];        // Q^N      (Ps of migration.cu:76)
-    float* Y = fld_[(N + 1) % 2];  // Q^{N-1}  (Psold)
-    float* R0 = fld_[2];
-    float* R1 = fld_[3];
+    float* X = fwd_cur_;  // Q^N      (Ps of migration.cu:76)
+    float* Y = fwd_old_;  // Q^{N-1}  (Psold)
+    float* free_buf[2];
+    int nf = 0;
+    for (float* b : fld_)
+        if (b != X && b != Y && nf < 2) free_buf[nf++] = b;
+    float* R0 = free_buf[0];
+    float* R1 = free_buf[1];
     const size_t bytes = (size_t)ns * fs * sizeof(float);
     check(cudaMemsetAsync(R0, 0, bytes, st_), "memset Pr");
     check(cudaMemsetAsync(R1, 0, bytes, st_), "memset Prold");
@@ -497,8 +763,14 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
             launch_bwd_step(a, gradient, grid, st_);
         }
     };
-    const long long key = ((long long)(gradient ? kBwdGradient : kBwdImage) * 8 + 4 + (&g == &abc_ ? 0 : 1)) *
-                              1000000LL + ns;
+    int xi = 0, yi = 0;
+    for (int k = 0; k < kBufFields; ++k) {
+        if (fld_[k] == X) xi = k;
+        if (fld_[k] == Y) yi = k;
+    }
+    const long long key =
+        (((long long)(gradient ? kBwdGradient : kBwdImage) * 8 + 4 + (&g == &abc_ ? 0 : 1)) * 16 + xi * 4 + yi) *
+            1000000LL + ns;
     if (use_graphs_) {
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {

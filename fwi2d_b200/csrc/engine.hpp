@@ -7,6 +7,7 @@
 // whole nt+tlag step loop is captured once per (propagation kind, batch size)
 // as a CUDA graph and replayed for every batch.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -97,9 +98,27 @@ private:
                      bool record, float* d_seis);
     void run_backward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride,
                       bool gradient, const float* d_series);
+    // forward-kernel choice for (grid, batch size, ABC): the simple tiled kernel
+    // (k_stencil.cu) or a persistent TMA variant (k_fwd_tma.cu), autotuned
+    struct FwdPlan {
+        int kind = 0;                 // 0 simple, 1 TMA
+        FwdTmaConfig cfg{1, 32, 2};
+        FwdTmaConfig tail{1, 32, 2};  // T = 1 variant for an odd last step
+        int grid = 0, tail_grid = 0;
+        double us_per_step = 0;
+    };
+    FwdPlan fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel, long long vel_stride);
+    const CUtensorMap& tmap(const float* base, const Grid& g, int nshots, int boxz, int boxx);
+    void upload_tile_base(const Grid& g, int ns, int tx);
+    void launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, const Tables& t, int ns, const float* vel,
+                             long long vel_stride, bool abc, float* cur, float* old, float* out1, float* out2, int tt,
+                             bool record, float* d_seis);
+    double time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                              long long vel_stride, bool abc);
     void check(cudaError_t e, const char* what);
     void sync(const char* what);
     void check_finite(const float* d, size_t n, const char* what);
+    int h_shot_nxx(const Grid& g, int /*batch-local shot*/) const { return g.nxx; }
     void ensure_rbc_base();
     double residual_of(int s0, int ns, const float* d_obs, const float* d_cal, float* d_res);
 
@@ -161,6 +180,18 @@ private:
     // time-loop graphs, key = (kind, grid, batch size)
     std::map<long long, cudaGraphExec_t> graphs_;
     bool use_graphs_ = true;
+    // TMA forward path
+    std::map<std::string, CUtensorMap> tmaps_;
+    std::map<long long, FwdPlan> plans_;
+    int* d_tile_base_ = nullptr;
+    int* d_err_ = nullptr;
+    int sm_count_ = 0;
+    std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S
+    float* fwd_cur_ = nullptr;         // Q^N after run_forward
+    float* fwd_old_ = nullptr;         // Q^{N-1}
+public:
+    // plan used by the last forward propagation (for reporting)
+    std::string last_fwd_plan;
 };
 
 }  // namespace fwi

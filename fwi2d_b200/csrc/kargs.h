@@ -57,6 +57,33 @@ struct FwdArgs {
     int nt;
 };
 
+// Persistent TMA forward kernel (k_fwd_tma.cu): one or two time levels per
+// launch, written out of place.
+struct FwdTmaArgs {
+    const ShotDesc* shots;
+    const int* tile_base;     // batch-local prefix sums of tiles per shot (ns+1)
+    int ns, ntz;              // shots in the batch, 128-row tiles per column
+    int ldz, nzz, nb;
+    long long fstride;
+    int vel_shared;           // 1: one velocity for all shots (tensor map of 1 shot)
+    float dt2idh2;
+    const float* b1d;         // ABC profile or NULL
+    InjTable inj;             // source table; sample1 / sample2 below
+    int sample1, sample2;     // wavelet samples added to Q^{t+1}, Q^{t+2}; -1 none
+    InjTable rec;             // receiver table (colptr, z, soff) of the batch
+    float* seis;              // trace-major seismograms, NULL when not recording
+    int rec_sample0, rec_sample1;  // samples recorded from Q^t and Q^{t+1}; -1 none
+    float* out1;              // Q^{t+1}
+    float* out2;              // Q^{t+2} (two-level launches)
+    int* err;                 // raised when a bounded wait gives up
+};
+
+struct FwdTmaConfig {
+    int T;    // time levels per launch (1 or 2)
+    int TX;   // tile columns
+    int S;    // pipeline stages
+};
+
 struct BwdArgs {
     const ShotDesc* shots;
     const float* vel;

@@ -1,5 +1,6 @@
 // kernels.h — launch wrappers of the device kernels (all enqueue on `st`).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -13,6 +14,18 @@ namespace fwi {
 dim3 step_grid(int ldz, int max_nxx, int nshots);
 void launch_fwd_step(const FwdArgs& a, dim3 grid, cudaStream_t st);
 void launch_bwd_step(const BwdArgs& a, bool gradient, dim3 grid, cudaStream_t st);
+
+// ---- k_fwd_tma.cu --------------------------------------------------------------
+int fwd_tma_rows();                                   // rows per tile (128)
+bool fwd_tma_supported(const FwdTmaConfig& c);
+size_t fwd_tma_smem(const FwdTmaConfig& c);           // dynamic shared memory bytes
+int fwd_tma_box_cur_z(const FwdTmaConfig& c);
+int fwd_tma_box_cur_x(const FwdTmaConfig& c);
+int fwd_tma_box_pt_z(const FwdTmaConfig& c);
+int fwd_tma_box_pt_x(const FwdTmaConfig& c);
+cudaError_t fwd_tma_configure(int* ctas_per_sm_out, const FwdTmaConfig& c);
+cudaError_t launch_fwd_tma(const FwdTmaConfig& c, const CUtensorMap& m_cur, const CUtensorMap& m_old,
+                           const CUtensorMap& m_vel, const FwdTmaArgs& a, int grid, cudaStream_t st);
 
 // ---- k_rbc.cu ----------------------------------------------------------------
 struct BumpDev { float xc, zc, r, A, factor; };

@@ -178,6 +178,9 @@ int  fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, 
                           void* stream);
 
 /* ---- timing / diagnostics ----------------------------------------------- */
+/* Text description of the forward-step kernel the autotuner chose for the last
+ * propagation (e.g. "tma T=2 TX=16 S=2 grid=148"). */
+int  fwi_describe(fwi_ctx* ctx, char* buf, size_t len);
 /* Kernel launches issued by the context since creation (or the last reset). */
 int  fwi_launch_count(fwi_ctx* ctx, long long* count, int reset);
 

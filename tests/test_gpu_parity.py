@@ -94,6 +94,35 @@ def test_set_model_and_cfl(case):
         assert e.value.code == -1
 
 
+VARIANTS = ["simple", "tma:1,32,2", "tma:1,32,3", "tma:1,16,3", "tma:1,16,4", "tma:2,32,2", "tma:2,16,2",
+            "tma:2,16,3"]
+
+
+@pytest.mark.parametrize("nt", [500, 501])  # nt + tlag odd (T = 2 ends with a one-level launch) and even
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_forward_kernel_variants_vs_oracle(tmp_path, variant, nt):
+    c, vp = synth.small_case(tmp_path, nt=nt, fwd_kernel=variant)
+    with api.Context(c.params, api.MODE_MODELING) as ctx:
+        seis = ctx.model_survey()
+    ref = _oracle_modeling(c, vp, 20, 0.004, 64)
+    for s in range(len(c.sx)):
+        assert rel_l2(seis[s], ref[s]) < RTOL, (variant, s)
+        assert np.all(seis[s][0] == 0.0)
+
+
+def test_forward_variants_agree_on_wide_grid(tmp_path):
+    """Several tiles per column and per shot, receivers across tile borders."""
+    outs = {}
+    for v in ("simple", "tma:1,32,2", "tma:2,16,2", "tma:2,32,2"):
+        c, vp = synth.small_case(tmp_path / v.replace(":", "_").replace(",", "_"), nz=260, nx=300, nt=300,
+                                 nshots=4, nrec=77, fwd_kernel=v)
+        with api.Context(c.params, api.MODE_MODELING) as ctx:
+            outs[v] = ctx.model_survey()
+    base = outs["simple"]
+    for v, o in outs.items():
+        assert rel_l2(o, base) < 1e-5, v
+
+
 # ---------------------------------------------------------------------------- random boundary
 def test_random_boundary_bit_exact(case):
     c, vp = case
@@ -115,8 +144,10 @@ def _rtm_data(c, vp):
     return np.stack(_oracle_modeling(c, vp, 20, 0.004, 64)).astype(np.float32)
 
 
-def test_rtm_vs_oracle(case):
-    c, vp = case
+@pytest.mark.parametrize("variant", ["auto", "simple", "tma:2,16,2", "tma:1,32,2"])
+def test_rtm_vs_oracle(case, tmp_path, variant):
+    c0, vp = case
+    c, _ = synth.small_case(tmp_path, fwd_kernel=variant)
     smooth = synth.smooth_model(vp, c.dh, 40.0)
     data = _rtm_data(c, vp)
     with api.Context(c.params, api.MODE_MIGRATION) as ctx:
