@@ -198,7 +198,7 @@ def profile_case():
     case, _ = synth.config2(d, seed=2, nt=40)
     with api.Context(case.params, api.MODE_MODELING) as ctx:
         ctx.model_survey_raw()
-    print("profile case done")
+        print("profile case done:", ctx.describe())
 
 
 def main():

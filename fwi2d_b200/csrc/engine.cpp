@@ -463,7 +463,11 @@ void Engine::upload_tile_base(const Grid& g, int ns, int tx) {
 void Engine::launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, const Tables& t, int ns,
                                  const float* vel, long long vel_stride, bool abc, float* cur, float* old,
                                  float* out1, float* out2, int tt, bool record, float* d_seis) {
-    const FwdTmaConfig& c = two ? p.cfg : p.tail;
+    // a one-level plan always runs its own variant; a two-level plan ends an
+    // odd step count with its one-level tail variant
+    const bool main_cfg = two || p.cfg.T == 1;
+    const FwdTmaConfig& c = main_cfg ? p.cfg : p.tail;
+    const int launch_grid = main_cfg ? p.grid : p.tail_grid;
     FwdTmaArgs a;
     a.shots = d_batch_;
     a.tile_base = d_tile_base_;
@@ -489,7 +493,7 @@ void Engine::launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, cons
     const CUtensorMap& mc = tmap(cur, g, batch_, fwd_tma_box_cur_z(c), fwd_tma_box_cur_x(c));
     const CUtensorMap& mo = tmap(old, g, batch_, fwd_tma_box_pt_z(c), fwd_tma_box_pt_x(c));
     const CUtensorMap& mv = tmap(vel, g, vel_stride ? batch_ : 1, fwd_tma_box_pt_z(c), fwd_tma_box_pt_x(c));
-    check(launch_fwd_tma(c, mc, mo, mv, a, two ? p.grid : p.tail_grid, st_), "forward TMA launch");
+    check(launch_fwd_tma(c, mc, mo, mv, a, launch_grid, st_), "forward TMA launch");
 }
 
 double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
@@ -582,6 +586,7 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
     }
     FwdPlan best;
     double best_us = 1e30;
+    std::ostringstream log;
     for (auto& c : cands) {
         if (c.kind < 0) continue;
         if (cands.size() == 1) {
@@ -589,12 +594,15 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
             break;
         }
         c.us_per_step = time_fwd_candidate(c, g, t, ns, vel, vel_stride, abc);
+        if (c.kind == 0) log << " simple=" << c.us_per_step;
+        else log << " tma" << c.cfg.T << "," << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
         if (c.us_per_step < best_us) {
             best_us = c.us_per_step;
             best = c;
         }
     }
     sync("forward autotune");
+    best.tuning = log.str();
     plans_[key] = best;
     return best;
 }
@@ -607,6 +615,7 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
         std::ostringstream d;
         if (plan.kind == 0) d << "simple";
         else d << "tma T=" << plan.cfg.T << " TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
+        if (!plan.tuning.empty()) d << " | us/step:" << plan.tuning;
         last_fwd_plan = d.str();
     }
     float* B[4] = {fld_[0], fld_[1], fld_[2], fld_[3]};

@@ -106,6 +106,7 @@ private:
         FwdTmaConfig tail{1, 32, 2};  // T = 1 variant for an odd last step
         int grid = 0, tail_grid = 0;
         double us_per_step = 0;
+        std::string tuning;           // autotuner timings of all candidates
     };
     FwdPlan fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel, long long vel_stride);
     const CUtensorMap& tmap(const float* base, const Grid& g, int nshots, int boxz, int boxx);

@@ -6,7 +6,7 @@
 //     Q^{t+1} = d * (v^2 dt^2/dh^2 * L(Q^t) + 2 Q^t - d * Q^{t-1}) + s_{t+1}
 // with the receivers recording d * Q^t.
 //
-// Structure (B200): one CTA per SM walks a list of 128-row x TX-column tiles
+// Structure (B200): persistent CTAs walk a list of 128-row x TX-column tiles
 // of all shots of the batch.  Thread 0 issues cp.async.bulk.tensor loads of
 // the next STAGES tiles (Q^t with its halo, Q^{t-1} and v) onto an mbarrier per
 // stage, so the memory system always has whole tiles in flight while the
@@ -23,6 +23,7 @@
 
 #include "kargs.h"
 #include "kernels.h"
+#include "stencil.cuh"
 #include "tma.cuh"
 
 namespace fwi {
@@ -49,66 +50,6 @@ struct Geom {
     static_assert(CZ <= 256 && CX <= 256, "TMA box extent");
 };
 
-__device__ __forceinline__ float el(const float4& v, int e) {
-    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
-}
-
-// dh^2 * Laplacian at rows r..r+3 (r % 4 == 0) of column c of a shared tile
-// whose columns hold LD floats.
-template <int LD>
-__device__ __forceinline__ void lap4(const float* t, int r, int c, float out[4]) {
-    const float c0 = (float)(-2.0 * kFDM5), c1 = (float)kFDM4, c2 = (float)(-kFDM3), c3 = (float)kFDM2,
-                c4 = (float)(-kFDM1);
-    const float* col = t + c * LD + r;
-    const float4 up = *reinterpret_cast<const float4*>(col - 4);
-    const float4 own = *reinterpret_cast<const float4*>(col);
-    const float4 dn = *reinterpret_cast<const float4*>(col + 4);
-    const float z[12] = {up.x, up.y, up.z, up.w, own.x, own.y, own.z, own.w, dn.x, dn.y, dn.z, dn.w};
-    float4 xm[4], xp[4];
-#pragma unroll
-    for (int k = 1; k <= 4; ++k) {
-        xm[k - 1] = *reinterpret_cast<const float4*>(col - k * LD);
-        xp[k - 1] = *reinterpret_cast<const float4*>(col + k * LD);
-    }
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const float s1 = (el(xm[0], e) + el(xp[0], e)) + (z[e + 3] + z[e + 5]);
-        const float s2 = (el(xm[1], e) + el(xp[1], e)) + (z[e + 2] + z[e + 6]);
-        const float s3 = (el(xm[2], e) + el(xp[2], e)) + (z[e + 1] + z[e + 7]);
-        const float s4 = (el(xm[3], e) + el(xp[3], e)) + (z[e + 0] + z[e + 8]);
-        float l = c4 * s4;
-        l = fmaf(c3, s3, l);
-        l = fmaf(c2, s2, l);
-        l = fmaf(c1, s1, l);
-        out[e] = fmaf(c0, z[e + 4], l);
-    }
-}
-
-// Cerjan damper in closed form (see k_stencil.cu); i, j inside the grid.
-__device__ __forceinline__ float damper(const float* __restrict__ b1d, int nb, int i, int j, int nzz, int nxx) {
-    const int iz = i < nb ? i : (i >= nzz - nb ? nzz - 1 - i : -1);
-    const int jx = j < nb ? j : (j >= nxx - nb ? nxx - 1 - j : -1);
-    const float dz = iz >= 0 ? __ldg(b1d + iz) : 1.0f;
-    const float dx = jx >= 0 ? __ldg(b1d + jx) : 1.0f;
-    return (iz >= 0 && jx >= 0) ? (dz + dx) - 1.0f : dz * dx;
-}
-
-// Source amplitude added at rows z..z+3 of column j (j inside the grid).
-__device__ __forceinline__ void inject4(const InjTable& inj, int sample, int col_off, int j, int z, float v[4]) {
-    if (sample < 0) return;
-    const int kb = __ldg(inj.colptr + col_off + j), ke = __ldg(inj.colptr + col_off + j + 1);
-    for (int k = kb; k < ke; ++k) {
-        const int dz = __ldg(inj.z + k) - z;
-        if (dz >= 0 && dz < 4) {
-            const float amp = inj.scale * __ldg(inj.series + __ldg(inj.soff + k) + sample);
-            if (dz == 0) v[0] += amp;
-            else if (dz == 1) v[1] += amp;
-            else if (dz == 2) v[2] += amp;
-            else v[3] += amp;
-        }
-    }
-}
-
 struct TileInfo {
     int s, x0, z0;
 };
@@ -128,6 +69,78 @@ __device__ __forceinline__ TileInfo decode(const FwdTmaArgs& a, int tile, int tx
     return ti;
 }
 
+// Everything a pass over one staged tile needs.
+struct Tile {
+    const float* cur;   // Q^t with an H-cell halo
+    const float* old;   // Q^{t-1} with an (H-4)-cell halo
+    const float* vel;   // v with an (H-4)-cell halo
+    float* mid;         // Q^{t+1} with a 4-cell ring (T = 2)
+    TileInfo ti;
+    int nxx, col_off;
+    bool has_src;
+};
+
+// T = 2: Q^{t+1} on the tile and its 4-cell ring, runs of 4 columns.
+template <int T, int TX, bool DAMP, bool EDGE>
+__device__ __forceinline__ void mid_pass(const FwdTmaArgs& a, const Tile& t) {
+    using G = Geom<T, TX>;
+    constexpr int QZ = G::MZ / 4;
+    constexpr int RUNS = G::MX / 4;
+    for (int w = threadIdx.x; w < QZ * RUNS; w += kNT) {
+        const int q = w % QZ, c0 = (w / QZ) * 4;
+        const int gz = t.ti.z0 - 4 + 4 * q;
+        const st::Rows rows = st::rows_info(DAMP ? a.b1d : nullptr, a.nb, gz, a.nzz);
+        float l[4][4];
+        float4 qq[4];
+        st::lap_run<G::CZ, 4>(t.cur, 4 * q + 4, c0 + 4, l, qq);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int c = c0 + m, gx = t.ti.x0 - 4 + c;
+            const float4 oo = *reinterpret_cast<const float4*>(t.old + c * G::PZ + 4 * q);
+            const float4 vv = *reinterpret_cast<const float4*>(t.vel + c * G::PZ + 4 * q);
+            const st::Col col =
+                (DAMP || EDGE) ? st::col_info(DAMP ? a.b1d : nullptr, a.nb, gx, t.nxx) : st::Col{1.0f, false, true};
+            float4 out = st::update4<DAMP, EDGE>(l[m], qq[m], oo, vv, a.dt2idh2, rows, col);
+            if (t.has_src && gx >= 0 && gx < t.nxx) st::inject4(a.inj, a.sample1, t.col_off, gx, gz, out);
+            *reinterpret_cast<float4*>(t.mid + c * G::MZ + 4 * q) = out;
+        }
+    }
+}
+
+// Last level of the launch on the tile: thread (lane, warp) owns rows
+// z0+4*lane .. +3 of the warp's TX/8 consecutive columns.
+template <int T, int TX, bool DAMP, bool EDGE>
+__device__ __forceinline__ void final_pass(const FwdTmaArgs& a, const Tile& t) {
+    using G = Geom<T, TX>;
+    constexpr int CPW = TX / 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int z = t.ti.z0 + 4 * lane;
+    if (z >= a.ldz) return;
+    const st::Rows rows = st::rows_info(DAMP ? a.b1d : nullptr, a.nb, z, a.nzz);
+    const int c0 = warp * CPW;
+    float l[CPW][4];
+    float4 qq[CPW];
+    if (T == 2) st::lap_run<G::MZ, CPW>(t.mid, 4 * lane + 4, c0 + 4, l, qq);
+    else st::lap_run<G::CZ, CPW>(t.cur, 4 * lane + 4, c0 + 4, l, qq);
+#pragma unroll
+    for (int m = 0; m < CPW; ++m) {
+        const int c = c0 + m;
+        const int gx = t.ti.x0 + c;
+        if (gx >= t.nxx) break;
+        const size_t goff = (size_t)t.ti.s * a.fstride + (size_t)gx * a.ldz + z;
+        if (T == 2) *reinterpret_cast<float4*>(a.out1 + goff) = qq[m];  // Q^{t+1} on the tile
+        const float4 oo = (T == 2) ? *reinterpret_cast<const float4*>(t.cur + (c + 8) * G::CZ + 4 * lane + 8)
+                                   : *reinterpret_cast<const float4*>(t.old + c * G::PZ + 4 * lane);
+        const float4 vv =
+            *reinterpret_cast<const float4*>(t.vel + (c + G::H - 4) * G::PZ + 4 * lane + (G::H - 4));
+        const st::Col col =
+            (DAMP || EDGE) ? st::col_info(DAMP ? a.b1d : nullptr, a.nb, gx, t.nxx) : st::Col{1.0f, false, true};
+        float4 out = st::update4<DAMP, EDGE>(l[m], qq[m], oo, vv, a.dt2idh2, rows, col);
+        if (t.has_src) st::inject4(a.inj, T == 2 ? a.sample2 : a.sample1, t.col_off, gx, z, out);
+        *reinterpret_cast<float4*>((T == 2 ? a.out2 : a.out1) + goff) = out;
+    }
+}
+
 template <int T, int TX, int S, bool ABC>
 __global__ void __launch_bounds__(kNT, 2)
     fwd_tma_kernel(const __grid_constant__ CUtensorMap m_cur, const __grid_constant__ CUtensorMap m_old,
@@ -135,7 +148,6 @@ __global__ void __launch_bounds__(kNT, 2)
     using G = Geom<T, TX>;
     extern __shared__ __align__(128) float smem[];
     __shared__ __align__(8) uint64_t full[S];
-    float* mid = smem + S * G::STAGE;
     const int tid = threadIdx.x;
     const int total = __ldg(a.tile_base + a.ns);
 
@@ -148,17 +160,17 @@ __global__ void __launch_bounds__(kNT, 2)
     }
     __syncthreads();
 
-    auto issue = [&](int tile, int st) {
+    auto issue = [&](int tile, int st_) {
         const TileInfo ti = decode(a, tile, TX);
-        float* base = smem + st * G::STAGE;
-        tma::mbar_arrive_expect_tx(&full[st], G::BYTES);
-        tma::load_3d(base, &m_cur, ti.z0 - G::H, ti.x0 - G::H, ti.s, &full[st]);
-        tma::load_3d(base + G::CUR, &m_old, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4), ti.s, &full[st]);
+        float* base = smem + st_ * G::STAGE;
+        tma::mbar_arrive_expect_tx(&full[st_], G::BYTES);
+        tma::load_3d(base, &m_cur, ti.z0 - G::H, ti.x0 - G::H, ti.s, &full[st_]);
+        tma::load_3d(base + G::CUR, &m_old, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4), ti.s, &full[st_]);
         tma::load_3d(base + G::CUR + G::PTW, &m_vel, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4),
-                     a.vel_shared ? 0 : ti.s, &full[st]);
+                     a.vel_shared ? 0 : ti.s, &full[st_]);
     };
 
-    int issued = 0;  // tiles issued by this CTA
+    int issued = 0;  // tiles issued by this CTA (thread 0)
     if (tid == 0)
         for (int k = 0; k < S; ++k) {
             const int tile = blockIdx.x + k * gridDim.x;
@@ -168,138 +180,74 @@ __global__ void __launch_bounds__(kNT, 2)
             }
         }
 
-    const int lane = tid & 31, warp = tid >> 5;
-    const float k2 = a.dt2idh2;
     int k = 0;
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
-        const int st = k % S;
-        const bool ok = tma::mbar_wait(&full[st], (uint32_t)((k / S) & 1));
+        const int stg = k % S;
+        const bool ok = tma::mbar_wait(&full[stg], (uint32_t)((k / S) & 1));
         if (!__syncthreads_and(ok)) {
             if (tid == 0) atomicExch(a.err, 1);
             break;
         }
-        const TileInfo ti = decode(a, tile, TX);
-        const ShotDesc sd = a.shots[ti.s];
-        const int nxx = sd.nxx;
-        const float* cur = smem + st * G::STAGE;
-        const float* old = cur + G::CUR;
-        const float* vel = old + G::PTW;
+        Tile t;
+        t.ti = decode(a, tile, TX);
+        const ShotDesc sd = a.shots[t.ti.s];
+        t.nxx = sd.nxx;
+        t.col_off = sd.col_off;
+        t.cur = smem + stg * G::STAGE;
+        t.old = t.cur + G::CUR;
+        t.vel = t.old + G::PTW;
+        t.mid = smem + S * G::STAGE;
+        t.has_src = (a.sample1 >= 0 || (T == 2 && a.sample2 >= 0)) &&
+                    st::has_points(a.inj, t.col_off, max(t.ti.x0 - 4, 0), min(t.ti.x0 + TX + 4, t.nxx));
+        const float* b1d = ABC ? a.b1d : nullptr;
 
         if (T == 2) {
-            // Q^{t+1} on the tile and a 4-cell ring around it
-            constexpr int QZ = G::MZ / 4;
-            for (int w = tid; w < QZ * G::MX; w += kNT) {
-                const int q = w % QZ, c = w / QZ;
-                const int gx = ti.x0 - 4 + c, gz = ti.z0 - 4 + 4 * q;
-                float out[4] = {0.f, 0.f, 0.f, 0.f};
-                if (gx >= 4 && gx < nxx - 4) {
-                    float l[4];
-                    lap4<G::CZ>(cur, 4 * q + 4, c + 4, l);
-                    const float4 qq = *reinterpret_cast<const float4*>(cur + (c + 4) * G::CZ + 4 * q + 4);
-                    const float4 oo = *reinterpret_cast<const float4*>(old + c * G::PZ + 4 * q);
-                    const float4 vv = *reinterpret_cast<const float4*>(vel + c * G::PZ + 4 * q);
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int i = gz + e;
-                        if (i >= 4 && i < a.nzz - 4) {
-                            const float v = el(vv, e);
-                            const float kk = k2 * (v * v);
-                            if (ABC) {
-                                const float d = damper(a.b1d, a.nb, i, gx, a.nzz, nxx);
-                                out[e] = d * (kk * l[e] + 2.0f * el(qq, e) - d * el(oo, e));
-                            } else {
-                                out[e] = kk * l[e] + 2.0f * el(qq, e) - el(oo, e);
-                            }
-                        }
-                    }
-                }
-                if (gx >= 0 && gx < nxx) inject4(a.inj, a.sample1, sd.col_off, gx, gz, out);
-                *reinterpret_cast<float4*>(mid + c * G::MZ + 4 * q) = make_float4(out[0], out[1], out[2], out[3]);
-            }
+            const bool inner = st::tile_inner(t.ti.z0 - 4, kTZ + 8, t.ti.x0 - 4, TX + 8, a.nzz, t.nxx);
+            const bool undamped = st::tile_undamped(b1d, a.nb, t.ti.z0 - 4, kTZ + 8, t.ti.x0 - 4, TX + 8, a.nzz, t.nxx);
+            if (inner && undamped) mid_pass<T, TX, false, false>(a, t);
+            else if (inner) mid_pass<T, TX, ABC, false>(a, t);
+            else mid_pass<T, TX, ABC, true>(a, t);
             __syncthreads();
         }
 
         // receivers owned by this tile: Q^t (and Q^{t+1}) from shared memory
         if ((a.rec_sample0 >= 0 || a.rec_sample1 >= 0) && a.seis) {
-            const int xe = min(ti.x0 + TX, nxx);
-            const int kb = __ldg(a.rec.colptr + sd.col_off + ti.x0), ke = __ldg(a.rec.colptr + sd.col_off + xe);
+            const int xe = min(t.ti.x0 + TX, t.nxx);
+            const int kb = __ldg(a.rec.colptr + t.col_off + t.ti.x0), ke = __ldg(a.rec.colptr + t.col_off + xe);
             for (int r = kb + tid; r < ke; r += kNT) {
                 const int z = __ldg(a.rec.z + r);
-                if (z < ti.z0 || z >= ti.z0 + kTZ) continue;
+                if (z < t.ti.z0 || z >= t.ti.z0 + kTZ) continue;
                 // column of the receiver: the last column whose colptr start is <= r
-                int lo = ti.x0, hi = xe;
+                int lo = t.ti.x0, hi = xe;
                 while (hi - lo > 1) {
                     const int m = (lo + hi) >> 1;
-                    if (__ldg(a.rec.colptr + sd.col_off + m) <= r) lo = m;
+                    if (__ldg(a.rec.colptr + t.col_off + m) <= r) lo = m;
                     else hi = m;
                 }
                 const int x = lo;
-                const float d = ABC ? damper(a.b1d, a.nb, z, x, a.nzz, nxx) : 1.0f;
+                const float d = ABC ? st::damp(st::rows_info(a.b1d, a.nb, z, a.nzz),
+                                               st::col_info(a.b1d, a.nb, x, t.nxx), 0)
+                                    : 1.0f;
                 const long long so = __ldg(a.rec.soff + r);
                 if (a.rec_sample0 >= 0)
-                    a.seis[so + a.rec_sample0] = d * cur[(x - ti.x0 + G::H) * G::CZ + (z - ti.z0 + G::H)];
+                    a.seis[so + a.rec_sample0] = d * t.cur[(x - t.ti.x0 + G::H) * G::CZ + (z - t.ti.z0 + G::H)];
                 if (T == 2 && a.rec_sample1 >= 0)
-                    a.seis[so + a.rec_sample1] = d * mid[(x - ti.x0 + 4) * G::MZ + (z - ti.z0 + 4)];
+                    a.seis[so + a.rec_sample1] = d * t.mid[(x - t.ti.x0 + 4) * G::MZ + (z - t.ti.z0 + 4)];
             }
         }
 
-        // last level of the launch on the tile
         {
-            const int p = lane;
-            const int z = ti.z0 + 4 * p;
-            constexpr int CPW = TX / 8;  // columns per warp
-            if (z < a.ldz) {
-#pragma unroll 1
-                for (int j = 0; j < CPW; ++j) {
-                    const int c = warp * CPW + j;
-                    const int gx = ti.x0 + c;
-                    if (gx >= nxx) break;
-                    float out[4] = {0.f, 0.f, 0.f, 0.f};
-                    const size_t goff = (size_t)ti.s * a.fstride + (size_t)gx * a.ldz + z;
-                    if (T == 2) {
-                        const float4 m1 = *reinterpret_cast<const float4*>(mid + (c + 4) * G::MZ + 4 * p + 4);
-                        *reinterpret_cast<float4*>(a.out1 + goff) = m1;
-                    }
-                    if (gx >= 4 && gx < nxx - 4) {
-                        float l[4];
-                        float4 qq, oo;
-                        if (T == 2) {
-                            lap4<G::MZ>(mid, 4 * p + 4, c + 4, l);
-                            qq = *reinterpret_cast<const float4*>(mid + (c + 4) * G::MZ + 4 * p + 4);
-                            oo = *reinterpret_cast<const float4*>(cur + (c + 8) * G::CZ + 4 * p + 8);
-                        } else {
-                            lap4<G::CZ>(cur, 4 * p + 4, c + 4, l);
-                            qq = *reinterpret_cast<const float4*>(cur + (c + 4) * G::CZ + 4 * p + 4);
-                            oo = *reinterpret_cast<const float4*>(old + c * G::PZ + 4 * p);
-                        }
-                        const float4 vv = *reinterpret_cast<const float4*>(vel + (c + G::H - 4) * G::PZ + 4 * p +
-                                                                             (G::H - 4));
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const int i = z + e;
-                            if (i >= 4 && i < a.nzz - 4) {
-                                const float v = el(vv, e);
-                                const float kk = k2 * (v * v);
-                                if (ABC) {
-                                    const float d = damper(a.b1d, a.nb, i, gx, a.nzz, nxx);
-                                    out[e] = d * (kk * l[e] + 2.0f * el(qq, e) - d * el(oo, e));
-                                } else {
-                                    out[e] = kk * l[e] + 2.0f * el(qq, e) - el(oo, e);
-                                }
-                            }
-                        }
-                    }
-                    inject4(a.inj, T == 2 ? a.sample2 : a.sample1, sd.col_off, gx, z, out);
-                    float* dst = (T == 2 ? a.out2 : a.out1) + goff;
-                    *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
-                }
-            }
+            const bool inner = st::tile_inner(t.ti.z0, kTZ, t.ti.x0, TX, a.nzz, t.nxx);
+            const bool undamped = st::tile_undamped(b1d, a.nb, t.ti.z0, kTZ, t.ti.x0, TX, a.nzz, t.nxx);
+            if (inner && undamped) final_pass<T, TX, false, false>(a, t);
+            else if (inner) final_pass<T, TX, ABC, false>(a, t);
+            else final_pass<T, TX, ABC, true>(a, t);
         }
-        __syncthreads();  // stage `st` (and the ring tile) are free again
+        __syncthreads();  // stage `stg` (and the ring tile) are free again
         if (tid == 0) {
             const int next = tile + S * gridDim.x;
             if (next < total) {
-                issue(next, st);
+                issue(next, stg);
                 ++issued;
             }
         }
