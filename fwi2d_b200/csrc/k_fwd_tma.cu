@@ -7,10 +7,12 @@
 // with the receivers recording d * Q^t.
 //
 // Structure (B200): persistent CTAs walk a list of 128-row x TX-column tiles
-// of all shots of the batch.  Thread 0 issues cp.async.bulk.tensor loads of
-// the next STAGES tiles (Q^t with its halo, Q^{t-1} and v) onto an mbarrier per
-// stage, so the memory system always has whole tiles in flight while the
-// CTA computes from shared memory.  With T = 2 the tile is loaded with an
+// of all shots of the batch.  A producer warp issues cp.async.bulk.tensor
+// loads of the next STAGES tiles (Q^t with its halo, Q^{t-1} and v), each
+// stage completing on a `full` mbarrier; eight consumer warps compute from
+// shared memory and release a stage on its `empty` mbarrier, so the memory
+// system always has whole tiles in flight and consumer warps never wait for
+// one another in one-level launches.  With T = 2 the tile is loaded with an
 // 8-cell halo, Q^{t+1} is computed on the tile plus a 4-cell ring in shared
 // memory, and Q^{t+2} on the tile: every launch advances two time levels and
 // writes both (out of place, into the other buffer pair), so a grid point
@@ -31,7 +33,8 @@ namespace fwi {
 namespace {
 
 constexpr int kTZ = 128;   // output rows per tile
-constexpr int kNT = 256;   // threads per CTA
+constexpr int kNC = 256;   // consumer threads (8 warps) per CTA
+constexpr int kNT = kNC + 32;  // + one producer warp
 
 template <int T, int TX>
 struct Geom {
@@ -69,6 +72,14 @@ __device__ __forceinline__ TileInfo decode(const FwdTmaArgs& a, int tile, int tx
     return ti;
 }
 
+// Per-tile facts the producer warp gathers (global loads off the consumers'
+// critical path) and publishes next to the tile's shared-memory stage.
+struct TileMeta {
+    int s, x0, z0, nxx, col_off;
+    int has_src;         // the tile or its 4-cell ring holds a source point
+    int rec_kb, rec_ke;  // receiver entries of the tile's columns
+};
+
 // Everything a pass over one staged tile needs.
 struct Tile {
     const float* cur;   // Q^t with an H-cell halo
@@ -86,7 +97,7 @@ __device__ __forceinline__ void mid_pass(const FwdTmaArgs& a, const Tile& t) {
     using G = Geom<T, TX>;
     constexpr int QZ = G::MZ / 4;
     constexpr int RUNS = G::MX / 4;
-    for (int w = threadIdx.x; w < QZ * RUNS; w += kNT) {
+    for (int w = threadIdx.x; w < QZ * RUNS; w += kNC) {
         const int q = w % QZ, c0 = (w / QZ) * 4;
         const int gz = t.ti.z0 - 4 + 4 * q;
         const st::Rows rows = st::rows_info(DAMP ? a.b1d : nullptr, a.nb, gz, a.nzz);
@@ -141,6 +152,8 @@ __device__ __forceinline__ void final_pass(const FwdTmaArgs& a, const Tile& t) {
     }
 }
 
+__device__ __forceinline__ void consumer_barrier() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
 template <int T, int TX, int S, bool ABC>
 __global__ void __launch_bounds__(kNT, 2)
     fwd_tma_kernel(const __grid_constant__ CUtensorMap m_cur, const __grid_constant__ CUtensorMap m_old,
@@ -148,57 +161,93 @@ __global__ void __launch_bounds__(kNT, 2)
     using G = Geom<T, TX>;
     extern __shared__ __align__(128) float smem[];
     __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t empty[S];
+    __shared__ TileMeta meta[S];
+    __shared__ int abort_flag;
     const int tid = threadIdx.x;
     const int total = __ldg(a.tile_base + a.ns);
 
     if (tid == 0) {
-        tma::prefetch_map(&m_cur);
-        tma::prefetch_map(&m_old);
-        tma::prefetch_map(&m_vel);
-        for (int k = 0; k < S; ++k) tma::mbar_init(&full[k], 1);
+        for (int k = 0; k < S; ++k) {
+            tma::mbar_init(&full[k], 1);
+            tma::mbar_init(&empty[k], kNC / 32);
+        }
+        abort_flag = 0;
         tma::fence_barrier_init();
     }
     __syncthreads();
 
-    auto issue = [&](int tile, int st_) {
-        const TileInfo ti = decode(a, tile, TX);
-        float* base = smem + st_ * G::STAGE;
-        tma::mbar_arrive_expect_tx(&full[st_], G::BYTES);
-        tma::load_3d(base, &m_cur, ti.z0 - G::H, ti.x0 - G::H, ti.s, &full[st_]);
-        tma::load_3d(base + G::CUR, &m_old, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4), ti.s, &full[st_]);
-        tma::load_3d(base + G::CUR + G::PTW, &m_vel, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4),
-                     a.vel_shared ? 0 : ti.s, &full[st_]);
-    };
-
-    int issued = 0;  // tiles issued by this CTA (thread 0)
-    if (tid == 0)
-        for (int k = 0; k < S; ++k) {
-            const int tile = blockIdx.x + k * gridDim.x;
-            if (tile < total) {
-                issue(tile, k);
-                ++issued;
+    if (tid >= kNC) {
+        // ---------------- producer warp: one elected lane issues the loads
+        if (tid != kNC) return;
+        tma::prefetch_map(&m_cur);
+        tma::prefetch_map(&m_old);
+        tma::prefetch_map(&m_vel);
+        int k = 0;
+        for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
+            const int stg = k % S;
+            if (k >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((k / S) - 1) & 1))) {
+                atomicExch(a.err, 1);
+                break;
             }
+            const TileInfo ti = decode(a, tile, TX);
+            const ShotDesc sd = a.shots[ti.s];
+            TileMeta& mt = meta[stg];
+            mt.s = ti.s;
+            mt.x0 = ti.x0;
+            mt.z0 = ti.z0;
+            mt.nxx = sd.nxx;
+            mt.col_off = sd.col_off;
+            mt.has_src = (a.sample1 >= 0 || (T == 2 && a.sample2 >= 0)) &&
+                         st::has_points(a.inj, sd.col_off, max(ti.x0 - 4, 0), min(ti.x0 + TX + 4, sd.nxx));
+            if ((a.rec_sample0 >= 0 || a.rec_sample1 >= 0) && a.seis) {
+                mt.rec_kb = __ldg(a.rec.colptr + sd.col_off + ti.x0);
+                mt.rec_ke = __ldg(a.rec.colptr + sd.col_off + min(ti.x0 + TX, sd.nxx));
+            } else {
+                mt.rec_kb = mt.rec_ke = 0;
+            }
+            float* base = smem + stg * G::STAGE;
+            // the arrive releases the meta writes to the consumers' acquiring wait
+            tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
+            tma::load_3d(base, &m_cur, ti.z0 - G::H, ti.x0 - G::H, ti.s, &full[stg]);
+            tma::load_3d(base + G::CUR, &m_old, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4), ti.s, &full[stg]);
+            tma::load_3d(base + G::CUR + G::PTW, &m_vel, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4),
+                         a.vel_shared ? 0 : ti.s, &full[stg]);
         }
+        // never leave copies in flight behind an exiting CTA: wait (bounded)
+        // for the last S loads issued
+        for (int kk = (k > S ? k - S : 0); kk < k; ++kk) tma::mbar_wait(&full[kk % S], (uint32_t)((kk / S) & 1));
+        return;
+    }
 
+    // -------------------- consumer warps
+    const int lane = tid & 31;
     int k = 0;
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
         const int stg = k % S;
-        const bool ok = tma::mbar_wait(&full[stg], (uint32_t)((k / S) & 1));
-        if (!__syncthreads_and(ok)) {
-            if (tid == 0) atomicExch(a.err, 1);
+        bool ok = tma::mbar_wait(&full[stg], (uint32_t)((k / S) & 1));
+        if (T == 2) {
+            // the ring tile is shared by all consumer warps: agree on going on
+            if (!ok) abort_flag = 1;
+            consumer_barrier();
+            ok = abort_flag == 0;
+        }
+        if (!ok) {
+            if (lane == 0) atomicExch(a.err, 1);
             break;
         }
+        const TileMeta mt = meta[stg];
         Tile t;
-        t.ti = decode(a, tile, TX);
-        const ShotDesc sd = a.shots[t.ti.s];
-        t.nxx = sd.nxx;
-        t.col_off = sd.col_off;
+        t.ti.s = mt.s;
+        t.ti.x0 = mt.x0;
+        t.ti.z0 = mt.z0;
+        t.nxx = mt.nxx;
+        t.col_off = mt.col_off;
         t.cur = smem + stg * G::STAGE;
         t.old = t.cur + G::CUR;
         t.vel = t.old + G::PTW;
         t.mid = smem + S * G::STAGE;
-        t.has_src = (a.sample1 >= 0 || (T == 2 && a.sample2 >= 0)) &&
-                    st::has_points(a.inj, t.col_off, max(t.ti.x0 - 4, 0), min(t.ti.x0 + TX + 4, t.nxx));
+        t.has_src = mt.has_src != 0;
         const float* b1d = ABC ? a.b1d : nullptr;
 
         if (T == 2) {
@@ -207,14 +256,13 @@ __global__ void __launch_bounds__(kNT, 2)
             if (inner && undamped) mid_pass<T, TX, false, false>(a, t);
             else if (inner) mid_pass<T, TX, ABC, false>(a, t);
             else mid_pass<T, TX, ABC, true>(a, t);
-            __syncthreads();
+            consumer_barrier();
         }
 
         // receivers owned by this tile: Q^t (and Q^{t+1}) from shared memory
-        if ((a.rec_sample0 >= 0 || a.rec_sample1 >= 0) && a.seis) {
+        if (mt.rec_kb < mt.rec_ke) {
             const int xe = min(t.ti.x0 + TX, t.nxx);
-            const int kb = __ldg(a.rec.colptr + t.col_off + t.ti.x0), ke = __ldg(a.rec.colptr + t.col_off + xe);
-            for (int r = kb + tid; r < ke; r += kNT) {
+            for (int r = mt.rec_kb + tid; r < mt.rec_ke; r += kNC) {
                 const int z = __ldg(a.rec.z + r);
                 if (z < t.ti.z0 || z >= t.ti.z0 + kTZ) continue;
                 // column of the receiver: the last column whose colptr start is <= r
@@ -243,18 +291,9 @@ __global__ void __launch_bounds__(kNT, 2)
             else if (inner) final_pass<T, TX, ABC, false>(a, t);
             else final_pass<T, TX, ABC, true>(a, t);
         }
-        __syncthreads();  // stage `stg` (and the ring tile) are free again
-        if (tid == 0) {
-            const int next = tile + S * gridDim.x;
-            if (next < total) {
-                issue(next, stg);
-                ++issued;
-            }
-        }
-    }
-    // a timed-out CTA still owns its in-flight copies: wait for them (bounded)
-    if (tid == 0 && k < issued) {
-        for (int kk = k; kk < issued; ++kk) tma::mbar_wait(&full[kk % S], (uint32_t)((kk / S) & 1));
+        __syncwarp();
+        if (lane == 0) tma::mbar_arrive(&empty[stg]);  // this warp is done with stage `stg`
+        if (T == 2) consumer_barrier();                // the ring tile is free again
     }
 }
 

@@ -56,24 +56,26 @@ __device__ __forceinline__ void load_tile(float4 (*t)[kSW], const float* __restr
     }
 }
 
-// Forward update of the 4 columns of thread (lane, ty) on a loaded tile.
+// Forward update of the 4 columns of thread (lane, ty) on a loaded tile, one
+// column at a time (few live registers, so 3-4 CTAs share an SM).
 template <bool DAMP, bool EDGE>
 __device__ __forceinline__ void fwd_columns(const FwdArgs& a, const float* tilef, const ShotDesc& sd, int nxx,
                                             int x0, int z, const float* vel, float* nxt, bool has_src,
                                             const st::Rows& rows) {
     const int lane = threadIdx.x, ty = threadIdx.y;
-    float l[4][4];
-    float4 q[4];
-    st::lap_run<kLD, 4>(tilef, 4 * lane + 4, 4 * ty + kH, l, q);
-#pragma unroll
+#pragma unroll 1
     for (int m = 0; m < 4; ++m) {
         const int j = x0 + 4 * ty + m;
         if (j >= nxx) break;
         const size_t off = (size_t)j * a.ldz + z;
         const float4 vv = __ldg(reinterpret_cast<const float4*>(vel + off));
         const float4 old = *reinterpret_cast<const float4*>(nxt + off);
-        const st::Col col = (DAMP || EDGE) ? st::col_info(DAMP ? a.b1d : nullptr, a.nb, j, nxx) : st::Col{1.0f, false, true};
-        float4 out = st::update4<DAMP, EDGE>(l[m], q[m], old, vv, a.dt2idh2, rows, col);
+        float l[1][4];
+        float4 q[1];
+        st::lap_run<kLD, 1>(tilef, 4 * lane + 4, 4 * ty + kH + m, l, q);
+        const st::Col col =
+            (DAMP || EDGE) ? st::col_info(DAMP ? a.b1d : nullptr, a.nb, j, nxx) : st::Col{1.0f, false, true};
+        float4 out = st::update4<DAMP, EDGE>(l[0], q[0], old, vv, a.dt2idh2, rows, col);
         if (has_src) st::inject4(a.inj, a.inj.sample, sd.col_off, j, z, out);
         *reinterpret_cast<float4*>(nxt + off) = out;
     }
@@ -104,13 +106,13 @@ __global__ void __launch_bounds__(kThreads) fwd_step_kernel(FwdArgs a) {
     }
     if (x0 >= nxx) return;
 
+    const int z = z0 + 4 * threadIdx.x;
+    const bool has_src = a.inj.sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + kTX, nxx));
     load_tile(tile, cur, a.ldz, nxx, z0, x0);
     __syncthreads();
 
-    const int z = z0 + 4 * threadIdx.x;
     if (z >= a.ldz) return;
     const float* tilef = reinterpret_cast<const float*>(&tile[0][0]);
-    const bool has_src = a.inj.sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + kTX, nxx));
     const bool inner = st::tile_inner(z0, 4 * kTZ4, x0, kTX, a.nzz, nxx);
     const bool undamped = !kABC || st::tile_undamped(a.b1d, a.nb, z0, 4 * kTZ4, x0, kTX, a.nzz, nxx);
     const st::Rows rows = st::rows_info(kABC ? a.b1d : nullptr, a.nb, z, a.nzz);
