@@ -34,6 +34,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp", "-Wa
 CU_SOURCES = {
     "k_stencil.cu": [],
     "k_fwd_tma.cu": [],
+    "k_fwd_loop.cu": [],
     "k_util.cu": [],
     "k_rbc.cu": ["-fmad=false"],
     "k_noalloc.cu": [],

@@ -242,6 +242,7 @@ void Engine::alloc_buffers() {
     for (int k = 0; k < kBufFields; ++k) fld_[k] = dalloc<float>(fsz, "wavefield");
     d_tile_base_ = dalloc<int>(batch_ + 1, "tile table");
     d_err_ = dalloc<int>(1, "error flag");
+    d_sync_ = dalloc<unsigned>(1, "grid barrier");
     check(cudaMemset(d_err_, 0, sizeof(int)), "memset error flag");
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -273,7 +274,7 @@ Engine::~Engine() {
     void* ptrs[] = {d_vp_, d_m_, d_vel_abc_, d_vel_rbc_base_, d_wavelet_, d_b1d_, d_batch_, d_batch_nxx_,
                     d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
-                    d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_};
+                    d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_, d_sync_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (st_) cudaStreamDestroy(st_);
@@ -521,26 +522,81 @@ double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables&
             a.rec_sample = -1;
             a.nt = nt_;
             launch_fwd_step(a, grid, st_);
-        } else {
+        } else if (p.kind == 1) {
             upload_tile_base(g, ns, p.cfg.TX);
             launch_fwd_tma_step(p, p.cfg.T == 2, g, t, ns, vel, vel_stride, abc, fld_[k % 2], fld_[(k + 1) % 2],
                                 fld_[2 + k % 2], fld_[3 - k % 2], 0, false, nullptr);
         }
     };
-    one(0);  // first use: module load, tensor maps
+    const int loop_steps = 4 * reps;  // a multi-level launch is timed over more levels
+    if (p.kind == 2) {
+        upload_tile_base(g, ns, p.cfg.TX);
+        launch_fwd_loop_levels(p, g, t, ns, vel, vel_stride, abc, false, nullptr, 0, 2);  // warm-up
+    } else {
+        one(0);  // first use: module load, tensor maps
+    }
     cudaEvent_t e0, e1;
     check(cudaEventCreate(&e0), "event");
     check(cudaEventCreate(&e1), "event");
     check(cudaEventRecord(e0, st_), "event record");
-    for (int k = 0; k < reps; ++k) one(k);
+    if (p.kind == 2) launch_fwd_loop_levels(p, g, t, ns, vel, vel_stride, abc, false, nullptr, 0, loop_steps);
+    else
+        for (int k = 0; k < reps; ++k) one(k);
     check(cudaEventRecord(e1, st_), "event record");
     check(cudaEventSynchronize(e1), "event sync");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const int steps = reps * (p.kind == 1 ? p.cfg.T : 1);
+    const int steps = p.kind == 2 ? loop_steps : reps * (p.kind == 1 ? p.cfg.T : 1);
     return 1e3 * ms / steps;
+}
+
+void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                                    long long vel_stride, bool abc, bool record, float* d_seis, int t_begin,
+                                    int t_end) {
+    const int TX = p.cfg.TX;
+    FwdLoopMaps maps;
+    for (int i = 0; i < 3; ++i) {
+        maps.cur[i] = tmap(fld_[i], g, batch_, fwd_tma_rows() + 8, TX + 8);
+        maps.pt[i] = tmap(fld_[i], g, batch_, fwd_tma_rows(), TX);
+    }
+    maps.cur[3] = maps.cur[2];
+    maps.pt[3] = maps.pt[2];
+    maps.vel = tmap(vel, g, vel_stride ? batch_ : 1, fwd_tma_rows(), TX);
+    FwdLoopArgs la;
+    FwdTmaArgs& a = la.base;
+    a.shots = d_batch_;
+    a.tile_base = d_tile_base_;
+    a.ns = ns;
+    a.ntz = (g.ldz + fwd_tma_rows() - 1) / fwd_tma_rows();
+    a.ldz = g.ldz;
+    a.nzz = g.nzz;
+    a.nb = g.nb;
+    a.fstride = g.fstride();
+    a.vel_shared = vel_stride == 0 ? 1 : 0;
+    a.dt2idh2 = dt_ * dt_ * idh2_;
+    a.b1d = abc ? d_b1d_ : nullptr;
+    a.inj = InjTable{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, -1, idh2_};
+    a.sample1 = a.sample2 = -1;
+    a.rec = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, nullptr, -1, 0.0f};
+    a.seis = record ? d_seis : nullptr;
+    a.rec_sample0 = a.rec_sample1 = -1;
+    a.out1 = a.out2 = nullptr;
+    a.err = d_err_;
+    la.t_begin = t_begin;
+    la.t_end = t_end;
+    la.nt = nt_;
+    la.tlag = tlag_;
+    la.record = record ? 1 : 0;
+    la.buf_cur = 0;
+    la.buf_old = 1;
+    la.buf_free = 2;
+    for (int i = 0; i < 4; ++i) la.bufs[i] = fld_[i];
+    la.sync = d_sync_;
+    check(cudaMemsetAsync(d_sync_, 0, sizeof(unsigned), st_), "memset grid barrier");
+    check(launch_fwd_loop(TX, p.cfg.S, maps, la, p.grid, st_), "multi-level forward launch");
+    ++launches_;
 }
 
 Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel,
@@ -569,6 +625,19 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         p.tail_grid = sm_count_ * ctas_t;
         return p;
     };
+    auto make_loop = [&](int TX, int S) {
+        FwdPlan p;
+        p.kind = 2;
+        p.cfg = FwdTmaConfig{1, TX, S};
+        int ctas = 0;
+        if (fwd_loop_configure(&ctas, TX, S) != cudaSuccess || ctas < 1) {
+            cudaGetLastError();
+            p.kind = -1;
+            return p;
+        }
+        p.grid = sm_count_ * ctas;
+        return p;
+    };
     std::vector<FwdPlan> cands;
     if (fwd_kernel_ == "simple") {
         cands.push_back(FwdPlan{});
@@ -577,12 +646,19 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         if (std::sscanf(fwd_kernel_.c_str() + 4, "%d,%d,%d", &T, &TX, &S) != 3 || !fwd_tma_supported({T, TX, S}))
             throw Error(FWI_ERR_PARAM, "fwd_kernel '" + fwd_kernel_ + "' is not a compiled TMA variant");
         cands.push_back(make(T, TX, S));
+    } else if (fwd_kernel_.rfind("loop:", 0) == 0) {
+        int TX = 0, S = 0;
+        if (std::sscanf(fwd_kernel_.c_str() + 5, "%d,%d", &TX, &S) != 2 || !fwd_loop_supported(TX, S))
+            throw Error(FWI_ERR_PARAM, "fwd_kernel '" + fwd_kernel_ + "' is not a compiled multi-level variant");
+        cands.push_back(make_loop(TX, S));
     } else if (fwd_kernel_ == "auto" || fwd_kernel_ == "tma") {
         if (fwd_kernel_ == "auto") cands.push_back(FwdPlan{});
         const int variants[][3] = {{1, 32, 2}, {1, 32, 3}, {1, 16, 3}, {1, 16, 4}, {2, 32, 2}, {2, 16, 2}, {2, 16, 3}};
         for (const auto& v : variants) cands.push_back(make(v[0], v[1], v[2]));
+        const int loops[][2] = {{32, 2}, {16, 3}, {16, 2}};
+        for (const auto& v : loops) cands.push_back(make_loop(v[0], v[1]));
     } else {
-        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma or tma:T,TX,S");
+        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma, tma:T,TX,S or loop:TX,S");
     }
     FwdPlan best;
     double best_us = 1e30;
@@ -595,6 +671,7 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         }
         c.us_per_step = time_fwd_candidate(c, g, t, ns, vel, vel_stride, abc);
         if (c.kind == 0) log << " simple=" << c.us_per_step;
+        else if (c.kind == 2) log << " loop" << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
         else log << " tma" << c.cfg.T << "," << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
         if (c.us_per_step < best_us) {
             best_us = c.us_per_step;
@@ -614,6 +691,7 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     {
         std::ostringstream d;
         if (plan.kind == 0) d << "simple";
+        else if (plan.kind == 2) d << "loop TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
         else d << "tma T=" << plan.cfg.T << " TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
         if (!plan.tuning.empty()) d << " | us/step:" << plan.tuning;
         last_fwd_plan = d.str();
@@ -625,6 +703,22 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     launch_inject_points(B[0], fs, d_batch_, ns, inj, g.ldz, st_);
     ++launches_;
     const int N = nt_ + tlag_;
+    if (plan.kind == 2) {
+        // every level in one cooperative launch: buffers rotate cur -> old, free -> cur
+        upload_tile_base(g, ns, plan.cfg.TX);
+        launch_fwd_loop_levels(plan, g, t, ns, vel, vel_stride, abc, record, d_seis, 0, N);
+        int c = 0, o = 1, f = 2;
+        for (int tt = 0; tt < N; ++tt) {
+            const int po = o;
+            o = c;
+            c = f;
+            f = po;
+        }
+        fwd_cur_ = B[c];
+        fwd_old_ = B[o];
+        check(cudaGetLastError(), "forward propagation");
+        return;
+    }
     const dim3 grid = step_grid(g.ldz, g.nxx, ns);
     const float dt2idh2 = dt_ * dt_ * idh2_;
     int launches_in_loop = 0;

@@ -116,6 +116,8 @@ private:
                              bool record, float* d_seis);
     double time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                               long long vel_stride, bool abc);
+    void launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                                long long vel_stride, bool abc, bool record, float* d_seis, int t_begin, int t_end);
     void check(cudaError_t e, const char* what);
     void sync(const char* what);
     void check_finite(const float* d, size_t n, const char* what);
@@ -186,6 +188,7 @@ private:
     std::map<long long, FwdPlan> plans_;
     int* d_tile_base_ = nullptr;
     int* d_err_ = nullptr;
+    unsigned* d_sync_ = nullptr;       // grid-barrier counter of the multi-level kernel
     int sm_count_ = 0;
     std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S
     float* fwd_cur_ = nullptr;         // Q^N after run_forward

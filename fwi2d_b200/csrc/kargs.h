@@ -78,6 +78,17 @@ struct FwdTmaArgs {
     int* err;                 // raised when a bounded wait gives up
 };
 
+// Cooperative multi-level forward kernel (k_fwd_loop.cu): levels
+// t_begin..t_end-1 in one launch, buffers rotating cur -> old, free -> cur.
+struct FwdLoopArgs {
+    FwdTmaArgs base;          // samples / outputs are set per level in the kernel
+    int t_begin, t_end;
+    int nt, tlag, record;
+    int buf_cur, buf_old, buf_free;  // indices into bufs at t_begin
+    float* bufs[4];
+    unsigned* sync;           // grid-barrier counter, zero at launch
+};
+
 struct FwdTmaConfig {
     int T;    // time levels per launch (1 or 2)
     int TX;   // tile columns

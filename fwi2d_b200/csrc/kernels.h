@@ -27,6 +27,19 @@ cudaError_t fwd_tma_configure(int* ctas_per_sm_out, const FwdTmaConfig& c);
 cudaError_t launch_fwd_tma(const FwdTmaConfig& c, const CUtensorMap& m_cur, const CUtensorMap& m_old,
                            const CUtensorMap& m_vel, const FwdTmaArgs& a, int grid, cudaStream_t st);
 
+// ---- k_fwd_loop.cu -------------------------------------------------------------
+// Tensor maps of the four field buffers (Q^t box with a 4-cell halo, pointwise
+// box) and of the velocity, passed by value to the cooperative kernel.
+struct FwdLoopMaps {
+    CUtensorMap cur[4];
+    CUtensorMap pt[4];
+    CUtensorMap vel;
+};
+bool fwd_loop_supported(int TX, int S);
+cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S);
+cudaError_t launch_fwd_loop(int TX, int S, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
+                            cudaStream_t st);
+
 // ---- k_rbc.cu ----------------------------------------------------------------
 struct BumpDev { float xc, zc, r, A, factor; };
 struct RbcArgs {
