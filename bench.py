@@ -190,12 +190,16 @@ def run_reference(args, rank, world):
     return line
 
 
-def profile_case():
-    """An L2-exceeding forward survey for ncu captures: the FWI survey's grid
-    (301x1701 + 100-cell ABC = 501x1901) with all 81 shots, nt 40 (277 steps)."""
+def profile_case(which: str = "large"):
+    """Forward surveys for ncu captures.  large: the FWI survey's grid
+    (301x1701 + 100-cell ABC = 501x1901) with all 81 shots, nt 40 (277 steps),
+    fields ~630 MB > L2.  small: the benchmark survey once (L2-resident)."""
     from fwi2d_b200 import api, synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_prof_"))
-    case, _ = synth.config2(d, seed=2, nt=40)
+    if which == "small":
+        case, _ = synth.config0(d, seed=0)
+    else:
+        case, _ = synth.config2(d, seed=2, nt=40)
     with api.Context(case.params, api.MODE_MODELING) as ctx:
         ctx.model_survey_raw()
         print("profile case done:", ctx.describe())
@@ -208,11 +212,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", action="store_true",
-                    help="for ncu: forward survey of 81 shots on 501x1901 (fields ~630 MB > L2), short time axis")
+    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small"],
+                    help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
+                         "time axis; small: the benchmark survey)")
     args = ap.parse_args()
     if args.profile:
-        return profile_case()
+        return profile_case(args.profile)
     rank, world, local = dist_env()
     args.warmup = max(args.warmup, 3)
 
