@@ -55,6 +55,14 @@ SIGNATURES = {
     "fwi_get_model": (C.c_int, [_P, _F]),
     "fwi_get_wavelet": (C.c_int, [_P, _F]),
     "fwi_get_indices": (C.c_int, [_P, C.c_int, _I, _I, _I]),
+    "fwi_get_window": (C.c_int, [_P, C.c_int, _I, _I]),
+    "fwi_set_shot_range": (C.c_int, [_P, C.c_int, C.c_int]),
+    "fwi_gradient_accumulate": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double)]),
+    "fwi_gradient_finish": (C.c_int, [_P]),
+    "fwi_accumulators": (C.c_int, [_P, C.POINTER(_F), C.POINTER(_F)]),
+    "fwi_trial_steps": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "fwi_parabola_step": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float)]),
+    "fwi_util_window": (C.c_int, [C.c_float, C.c_float, C.c_int, C.c_float, _I, _I]),
     "fwi_model_shot": (C.c_int, [_P, C.c_int, _F]),
     "fwi_model_survey": (C.c_int, [_P, _F]),
     "fwi_model_survey_dev": (C.c_int, [_P, _P]),
@@ -83,6 +91,8 @@ SIGNATURES = {
     "fwi_util_normal": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _F]),
     "fwi_residual_noalloc": (C.c_int, [_P, _P, _P, C.c_size_t, _P, _P]),
     "fwi_describe": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "fwi_fwd_timing": (C.c_int, [_P, C.c_int]),
+    "fwi_fwd_timing_read": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 
@@ -168,9 +178,19 @@ class Context:
         return buf.value.decode()
 
     def describe(self) -> str:
-        buf = C.create_string_buffer(256)
-        self._check(self._lib.fwi_describe(self._h, buf, 256))
+        buf = C.create_string_buffer(4096)
+        self._check(self._lib.fwi_describe(self._h, buf, 4096))
         return buf.value.decode()
+
+    def fwd_timing(self, enable: bool = True) -> None:
+        """Start (reset) or stop CUDA-event timing of the forward kernel."""
+        self._check(self._lib.fwi_fwd_timing(self._h, int(enable)))
+
+    def fwd_timing_read(self) -> tuple[float, int, int]:
+        """(device ms, forward-kernel launches, grid-point updates) since fwd_timing(True)."""
+        ms, n, u = C.c_double(), C.c_longlong(), C.c_longlong()
+        self._check(self._lib.fwi_fwd_timing_read(self._h, C.byref(ms), C.byref(n), C.byref(u)))
+        return ms.value, n.value, u.value
 
     def launches(self, reset: bool = False) -> int:
         c = C.c_longlong()
@@ -209,6 +229,12 @@ class Context:
         _i = lambda a: a.ctypes.data_as(_I)
         self._check(self._lib.fwi_get_indices(self._h, shot, _i(sxz), _i(rx), _i(rz)))
         return int(sxz[0]), int(sxz[1]), rx, rz
+
+    def window(self, shot: int) -> tuple[int, int]:
+        """Aperture window (c0, w) of a shot: model columns c0 .. c0+w-1."""
+        c0, w = C.c_int(), C.c_int()
+        self._check(self._lib.fwi_get_window(self._h, shot, C.byref(c0), C.byref(w)))
+        return c0.value, w.value
 
     # -- modeling: seismograms returned as (nt, nrec) per shot (trace-major on disk)
     def _seis_view(self, flat: np.ndarray, nshots: int) -> np.ndarray:
@@ -305,15 +331,46 @@ class Context:
         self._check(self._lib.fwi_optimization(self._h, f0, C.byref(s)))
         return s.value
 
+    # -- sharded inversion
+    def set_shot_range(self, s0: int, ns: int) -> None:
+        self._check(self._lib.fwi_set_shot_range(self._h, s0, ns))
+
+    def gradient_accumulate(self, with_gradient: bool = True) -> float:
+        s = C.c_double()
+        self._check(self._lib.fwi_gradient_accumulate(self._h, int(with_gradient), C.byref(s)))
+        return s.value
+
+    def gradient_finish(self) -> None:
+        self._check(self._lib.fwi_gradient_finish(self._h))
+
+    def accumulators(self) -> tuple[int, int, int]:
+        """(device address of the raw image / gradient, of the illumination, floats each)."""
+        a, b = _F(), _F()
+        self._check(self._lib.fwi_accumulators(self._h, C.byref(a), C.byref(b)))
+        d = self.dims
+        return C.cast(a, C.c_void_p).value, C.cast(b, C.c_void_p).value, d.nz * d.nx
+
+    def trial_steps(self) -> tuple[float, float]:
+        a1, a2 = C.c_float(), C.c_float()
+        self._check(self._lib.fwi_trial_steps(self._h, C.byref(a1), C.byref(a2)))
+        return a1.value, a2.value
+
+    def parabola_step(self, f0: float, f1: float, f2: float) -> float:
+        s = C.c_float()
+        self._check(self._lib.fwi_parabola_step(self._h, f0, f1, f2, C.byref(s)))
+        return s.value
+
     def update_model(self, step: float) -> np.ndarray:
         out = self._grid_out()
         self._check(self._lib.fwi_update_model(self._h, step, _fptr(out)))
         return self._as2d(out)
 
     def random_boundary(self, shot: int) -> np.ndarray:
+        """Random-boundary velocity of a shot on its RBC grid, (nzz, w + 2 nb)."""
         d = self.dims
         nb = d.rbc_nb
-        nzz, nxx = d.nz + 2 * nb, d.nx + 2 * nb
+        _, w = self.window(shot)
+        nzz, nxx = d.nz + 2 * nb, w + 2 * nb
         out = np.empty(nzz * nxx, np.float32)
         self._check(self._lib.fwi_random_boundary(self._h, shot, _fptr(out)))
         return out.reshape(nxx, nzz).T
@@ -351,6 +408,13 @@ def util_grid_index(coord: np.ndarray, dh: float, nb: int) -> np.ndarray:
     out = np.empty(c.size, np.int32)
     _util_check(lib().fwi_util_grid_index(c.size, _fptr(c), dh, nb, out.ctypes.data_as(_I)), "grid index")
     return out
+
+
+def util_window(xs: float, max_offset: float, nx: int, dh: float) -> tuple[int, int]:
+    """Aperture window (c0, w) of a source at xs for a maximum offset."""
+    c0, w = C.c_int(), C.c_int()
+    _util_check(lib().fwi_util_window(xs, max_offset, nx, dh, C.byref(c0), C.byref(w)), "window")
+    return c0.value, w.value
 
 
 def util_bumps(nxx: int, nzz: int, nb: int, dh: float, ratio: float, varVp: float, seed: int, shot: int) -> np.ndarray:

@@ -127,17 +127,27 @@ int fwi_get_indices(fwi_ctx* ctx, int shot, int* src_xz, int* rec_x, int* rec_z)
     return guarded(ctx, [&](fwi::Engine& e) { e.get_indices(shot, src_xz, rec_x, rec_z); });
 }
 
+int fwi_get_window(fwi_ctx* ctx, int shot, int* c0, int* w) {
+    if (!c0 || !w) return arg_error(ctx, "NULL window output");
+    return guarded(ctx, [&](fwi::Engine& e) { e.get_window(shot, c0, w); });
+}
+
 int fwi_model_shot(fwi_ctx* ctx, int shot, float* seis) {
     if (!seis) return arg_error(ctx, "NULL seismogram");
     return guarded(ctx, [&](fwi::Engine& e) { e.model_shots(shot, 1, seis, false); });
 }
 
 int fwi_model_survey(fwi_ctx* ctx, float* seis_all) {
-    return guarded(ctx, [&](fwi::Engine& e) { e.model_shots(0, e.dims().nsrc, seis_all, false); });
+    return guarded(ctx, [&](fwi::Engine& e) {
+        e.model_shots(e.range_s0(), e.range_n(), seis_all ? seis_all + e.survey_offset(e.range_s0()) : nullptr, false);
+    });
 }
 
 int fwi_model_survey_dev(fwi_ctx* ctx, float* d_seis_all) {
-    return guarded(ctx, [&](fwi::Engine& e) { e.model_shots(0, e.dims().nsrc, d_seis_all, true); });
+    return guarded(ctx, [&](fwi::Engine& e) {
+        e.model_shots(e.range_s0(), e.range_n(), d_seis_all ? d_seis_all + e.survey_offset(e.range_s0()) : nullptr,
+                      true);
+    });
 }
 
 int fwi_rtm_reset(fwi_ctx* ctx) {
@@ -151,12 +161,16 @@ int fwi_rtm_shot(fwi_ctx* ctx, int shot, const float* data) {
 
 int fwi_rtm_survey(fwi_ctx* ctx, const float* data_all) {
     if (!data_all) return arg_error(ctx, "NULL data");
-    return guarded(ctx, [&](fwi::Engine& e) { e.rtm_shots(0, e.dims().nsrc, data_all, false); });
+    return guarded(ctx, [&](fwi::Engine& e) {
+        e.rtm_shots(e.range_s0(), e.range_n(), data_all + e.survey_offset(e.range_s0()), false);
+    });
 }
 
 int fwi_rtm_survey_dev(fwi_ctx* ctx, const float* d_data_all) {
     if (!d_data_all) return arg_error(ctx, "NULL data");
-    return guarded(ctx, [&](fwi::Engine& e) { e.rtm_shots(0, e.dims().nsrc, d_data_all, true); });
+    return guarded(ctx, [&](fwi::Engine& e) {
+        e.rtm_shots(e.range_s0(), e.range_n(), d_data_all + e.survey_offset(e.range_s0()), true);
+    });
 }
 
 int fwi_rtm_image(fwi_ctx* ctx, float* image) {
@@ -183,6 +197,39 @@ int fwi_compute_gradient(fwi_ctx* ctx, int with_gradient, double* sum_res) {
         double s = e.compute_gradient(with_gradient != 0);
         if (sum_res) *sum_res = s;
     });
+}
+
+int fwi_set_shot_range(fwi_ctx* ctx, int s0, int ns) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.set_shot_range(s0, ns); });
+}
+
+int fwi_gradient_accumulate(fwi_ctx* ctx, int with_gradient, double* sum_res) {
+    return guarded(ctx, [&](fwi::Engine& e) {
+        double s = e.accumulate_gradient(with_gradient != 0);
+        if (sum_res) *sum_res = s;
+    });
+}
+
+int fwi_gradient_finish(fwi_ctx* ctx) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.finish_gradient(); });
+}
+
+int fwi_accumulators(fwi_ctx* ctx, float** a, float** b) {
+    if (!a || !b) return arg_error(ctx, "NULL output");
+    return guarded(ctx, [&](fwi::Engine& e) {
+        e.accumulators(a, b);
+        e.stream_sync();
+    });
+}
+
+int fwi_trial_steps(fwi_ctx* ctx, float* a1, float* a2) {
+    if (!a1 || !a2) return arg_error(ctx, "NULL output");
+    return guarded(ctx, [&](fwi::Engine& e) { e.trial_steps(a1, a2); });
+}
+
+int fwi_parabola_step(fwi_ctx* ctx, float f0, float f1, float f2, float* step) {
+    if (!step) return arg_error(ctx, "NULL step");
+    return guarded(ctx, [&](fwi::Engine& e) { *step = e.parabola_step(f0, f1, f2); });
 }
 
 int fwi_get_gradient(fwi_ctx* ctx, float* g) {
@@ -268,6 +315,22 @@ int fwi_util_bumps(int nxx, int nzz, int nb, float dh, float ratio, float varVp,
     return FWI_OK;
 }
 
+int fwi_util_window(float xs, float max_offset, int nx, float dh, int* c0, int* w) {
+    if (!c0 || !w || nx < 9 || !(dh > 0)) return FWI_ERR_ARG;
+    try {
+        fwi::Geometry g;
+        g.xsrc = {xs};
+        g.zsrc = {0.0f};
+        const auto win = fwi::aperture_windows(g, nx, dh, {max_offset});
+        *c0 = win[0].c0;
+        *w = win[0].w;
+        return FWI_OK;
+    } catch (const fwi::Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    }
+}
+
 int fwi_util_normal(uint64_t seed, uint32_t shot, uint32_t stream, uint64_t ctr, float* out) {
     if (!out) return FWI_ERR_ARG;
     *out = detm::normalf(detm::stream_key(seed, shot, stream), ctr);
@@ -293,6 +356,15 @@ int fwi_describe(fwi_ctx* ctx, char* buf, size_t len) {
 int fwi_launch_count(fwi_ctx* ctx, long long* count, int reset) {
     if (!count) return arg_error(ctx, "NULL count");
     return guarded(ctx, [&](fwi::Engine& e) { *count = e.launches(reset != 0); });
+}
+
+int fwi_fwd_timing(fwi_ctx* ctx, int enable) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.fwd_timing(enable != 0); });
+}
+
+int fwi_fwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates) {
+    if (!ms || !launches || !updates) return arg_error(ctx, "NULL output");
+    return guarded(ctx, [&](fwi::Engine& e) { e.fwd_timing_read(ms, launches, updates); });
 }
 
 }  // extern "C"

@@ -30,13 +30,23 @@ public:
 
     fwi_dims dims() const;
     cudaStream_t stream() const { return st_; }
-    void set_seed(uint64_t s) { seed_ = s; }
+    void stream_sync() { sync("stream"); }
+    // restarts the sequence of random boundaries (one per gradient pass)
+    void set_seed(uint64_t s) {
+        seed_ = s;
+        rbc_epoch_ = 0;
+    }
     long long launches(bool reset) { long long c = launches_; if (reset) launches_ = 0; return c; }
+    // forward-kernel timing (events around each forward propagation launch)
+    void fwd_timing(bool enable);
+    void fwd_timing_read(double* ms, long long* launches, long long* updates);
 
     void set_model(const float* vp_host);          // nz x nx
     void get_model(float* vp_host);
     void get_wavelet(float* w) const;
     void get_indices(int shot, int* src_xz, int* rec_x, int* rec_z) const;
+    // aperture window of a shot: model columns [c0, c0 + w)
+    void get_window(int shot, int* c0, int* w) const;
 
     // modeling
     void model_shots(int s0, int ns, float* seis_out, bool out_on_device);
@@ -48,6 +58,18 @@ public:
     // inversion
     void set_observed(const float* obs, bool on_device);
     double compute_gradient(bool with_gradient);
+    // sharded inversion: compute_gradient = accumulate_gradient (shots of the
+    // range, raw accumulators) + finish_gradient (post-processing)
+    void set_shot_range(int s0, int ns);
+    int range_s0() const { return range_s0_; }
+    int range_n() const { return range_n_; }
+    // float offset of shot s's seismogram in an all-shots buffer
+    size_t survey_offset(int s) const { return (size_t)s * nrec_ * nt_; }
+    double accumulate_gradient(bool with_gradient);
+    void finish_gradient();
+    void accumulators(float** a, float** b) const;
+    void trial_steps(float* a1, float* a2) const;
+    float parabola_step(float f0, float f1, float f2) const;
     void get_gradient(float* g_host);
     void get_gradient_raw(float* g_host, float* illum_host);
     double linesearch_trial(float alpha);
@@ -69,14 +91,18 @@ public:
 
 private:
     struct Grid {
-        int nb = 0, nxx = 0, nzz = 0, ldz = 0;
+        int nb = 0;
+        int nxx = 0;       // widest shot grid (window + 2 nb); every shot's when not windowed
+        int nzz = 0, ldz = 0;
+        int full_nxx = 0;  // nx + 2 nb: the padded whole model
         long long fstride() const { return (long long)ldz * nxx; }
     };
     // Per-grid shot tables (indices depend on nb).
     struct Tables {
         std::vector<ShotDesc> shots;       // one per survey shot
-        std::vector<int> src_x, src_z;     // grid indices
+        std::vector<int> src_x, src_z;     // grid indices on the padded whole model
         std::vector<int> rec_x, rec_z;     // per receiver (same for all shots)
+        std::vector<int> nxx;              // per shot: width of its grid
         int* d_rec_pt = nullptr;           // nsrc*nrec
         int* d_src_colptr = nullptr;       // nsrc*(nxx+1)
         int* d_src_z = nullptr;
@@ -91,6 +117,10 @@ private:
     void free_tables(Tables* t);
     void alloc_buffers();
     void upload_batch(const Tables& t, int s0, int ns);
+    void setup_windows();
+    // velocity of the batch's shots on the RBC grid: the shared padded model,
+    // or (windowed) every shot's window padded by edge replication
+    void rbc_base(int s0, int ns, const float** base, long long* stride);
     void expand_to(const Grid& g, const float* d_model_interior, float* d_out);
     void build_rbc(int s0, int ns);
     // forward propagation of the current batch (fields end in fld_[0..1])
@@ -109,7 +139,8 @@ private:
         std::string tuning;           // autotuner timings of all candidates
     };
     FwdPlan fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel, long long vel_stride);
-    const CUtensorMap& tmap(const float* base, const Grid& g, int nshots, int boxz, int boxx);
+    const CUtensorMap& tmap(const float* base, const Grid& g, int nshots, int boxz, int boxx,
+                            bool whole_model = false);
     void upload_tile_base(const Grid& g, int ns, int tx);
     void launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, const Tables& t, int ns, const float* vel,
                              long long vel_stride, bool abc, float* cur, float* old, float* out1, float* out2, int tt,
@@ -117,11 +148,29 @@ private:
     double time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                               long long vel_stride, bool abc);
     void launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
-                                long long vel_stride, bool abc, bool record, float* d_seis, int t_begin, int t_end);
+                                long long vel_stride, bool abc, bool record, float* d_seis, int t_begin, int t_end,
+                                long long timed_updates = -1);
+    // events of one timed forward region: begin is recorded before the
+    // region's kernel(s), end after them
+    struct TimedRegion {
+        cudaEvent_t begin = nullptr, end = nullptr;
+        long long launches = 0, updates = 0;
+    };
+    cudaEvent_t timing_event();
+    void timing_begin(TimedRegion* r);
+    void timing_end(TimedRegion* r, long long launches, long long updates);
     void check(cudaError_t e, const char* what);
     void sync(const char* what);
     void check_finite(const float* d, size_t n, const char* what);
-    int h_shot_nxx(const Grid& g, int /*batch-local shot*/) const { return g.nxx; }
+    int h_shot_nxx(const Grid& g, int s /*batch-local shot*/) const {
+        return batch_t_ ? batch_t_->nxx[batch_s0_ + s] : g.nxx;
+    }
+    // padded grid points of a batch of ns shots (one time level)
+    long long batch_points(const Grid& g, int ns) const {
+        long long n = 0;
+        for (int s = 0; s < ns; ++s) n += (long long)g.nzz * h_shot_nxx(g, s);
+        return n;
+    }
     void ensure_rbc_base();
     double residual_of(int s0, int ns, const float* d_obs, const float* d_cal, float* d_res);
 
@@ -142,6 +191,15 @@ private:
     long long rbc_epoch_ = 0;
     int batch_ = 1;
     long long launches_ = 0;
+    int range_s0_ = 0, range_n_ = 0;    // shots of compute_gradient / linesearch_trial
+    // aperture windows
+    std::vector<Window> win_;
+    bool windowed_ = false;
+    int* d_full_win_ = nullptr;          // {0} and {nx}: the whole-model window
+    unsigned char* d_trace_keep_ = nullptr;  // per trace: receiver inside the shot's window
+    // batch being propagated (tables and first survey shot)
+    const Tables* batch_t_ = nullptr;
+    int batch_s0_ = 0;
 
     cudaStream_t st_ = nullptr;
     // model state
@@ -193,6 +251,12 @@ private:
     std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S
     float* fwd_cur_ = nullptr;         // Q^N after run_forward
     float* fwd_old_ = nullptr;         // Q^{N-1}
+    // forward-kernel timing
+    bool timing_ = false;
+    std::vector<TimedRegion> timed_;
+    std::vector<cudaEvent_t> event_pool_;
+    double timed_ms_ = 0;
+    long long timed_launches_ = 0, timed_updates_ = 0;
 public:
     // plan used by the last forward propagation (for reporting)
     std::string last_fwd_plan;

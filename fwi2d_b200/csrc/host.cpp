@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 
@@ -101,6 +102,45 @@ void read_floats(const std::string& path, float* dst, size_t n) {
     f.read(reinterpret_cast<char*>(dst), (std::streamsize)(n * sizeof(float)));
     if ((size_t)f.gcount() != n * sizeof(float))
         throw Error(FWI_ERR_IO, path + ": expected " + std::to_string(n) + " float32 values, file is shorter");
+}
+
+std::vector<float> read_text_floats(const std::string& path) {
+    std::vector<float> v;
+    for (std::string line : read_text_lines(path)) {
+        std::replace(line.begin(), line.end(), ',', ' ');
+        std::istringstream in(line);
+        std::string tok;
+        while (in >> tok) {
+            char* end = nullptr;
+            const float x = std::strtof(tok.c_str(), &end);
+            if (!end || *end != '\0') throw Error(FWI_ERR_PARAM, path + ": '" + tok + "' is not a number");
+            v.push_back(x);
+        }
+    }
+    return v;
+}
+
+std::vector<Window> aperture_windows(const Geometry& geo, int nx, float dh, const std::vector<float>& max_offset) {
+    const int ns = geo.nsrc();
+    std::vector<Window> win(ns, Window{0, nx});
+    if (max_offset.empty()) return win;
+    if ((int)max_offset.size() != ns)
+        throw Error(FWI_ERR_PARAM, "max offsets: " + std::to_string(max_offset.size()) + " values for " +
+                                       std::to_string(ns) + " shots");
+    for (int s = 0; s < ns; ++s) {
+        const double off = max_offset[s], xs = geo.xsrc[s];
+        if (!(off > 0)) throw Error(FWI_ERR_PARAM, "max offset of shot " + std::to_string(s + 1) + " must be positive");
+        int c0 = (int)std::floor((xs - off) / (double)dh);
+        int c1 = (int)std::ceil((xs + off) / (double)dh);
+        c0 = std::min(std::max(c0, 0), nx - 1);
+        c1 = std::min(std::max(c1, 0), nx - 1);
+        while (c1 - c0 + 1 < 9) {
+            if (c0 > 0) --c0;
+            if (c1 - c0 + 1 < 9 && c1 < nx - 1) ++c1;
+        }
+        win[s] = Window{c0, c1 - c0 + 1};
+    }
+    return win;
 }
 
 void write_floats(const std::string& path, const float* src, size_t n) {

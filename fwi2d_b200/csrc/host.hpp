@@ -56,6 +56,19 @@ struct Geometry {
 };
 Geometry read_geometry(const std::string& sps_path, const std::string& rps_path);
 
+// ---- aperture windows (batched uneven-aperture surveys) -----------------------
+// Not in the reference, which models every shot on the whole model.  Shot s
+// is modeled on the model columns [c0, c0 + w): the columns within
+// max_offset[s] of its source, c0 = floor((xs - off)/dh), c1 = ceil((xs + off)/dh),
+// both clamped to [0, nx); windows narrower than 9 columns are widened about
+// the source.  An empty max_offset gives every shot the whole model.
+struct Window {
+    int c0, w;
+};
+std::vector<Window> aperture_windows(const Geometry& geo, int nx, float dh, const std::vector<float>& max_offset);
+// Whitespace- or comma-separated floats of a text file ('#' lines skipped).
+std::vector<float> read_text_floats(const std::string& path);
+
 // ---- wavelet (modeling.cu:32-90) -------------------------------------------
 // Ricker of peak fmax/(3 sqrt(pi)) delayed by t0 = 2 sqrt(pi)/fmax, scaled by
 // 1e5, filtered by (i 2 pi f)^(1/2) in double precision and divided by nt.

@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(kNT, 2)
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
                     tma::load_3d(base, &maps.cur[c], ti.z0 - 4, ti.x0 - 4, ti.s, &full[stg]);
                     tma::load_3d(base + G::CUR, &maps.pt[o], ti.z0, ti.x0, ti.s, &full[stg]);
-                    tma::load_3d(base + G::CUR + G::PTW, &maps.vel, ti.z0, ti.x0, a.vel_shared ? 0 : ti.s,
-                                 &full[stg]);
+                    tma::load_3d(base + G::CUR + G::PTW, &maps.vel, ti.z0, ti.x0 + sd.vel_col,
+                                 a.vel_shared ? 0 : ti.s, &full[stg]);
                     issued = kk + 1;
                 }
                 if (!ok) {

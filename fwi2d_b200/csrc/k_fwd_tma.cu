@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kNT, 2)
             tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
             tma::load_3d(base, &m_cur, ti.z0 - G::H, ti.x0 - G::H, ti.s, &full[stg]);
             tma::load_3d(base + G::CUR, &m_old, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4), ti.s, &full[stg]);
-            tma::load_3d(base + G::CUR + G::PTW, &m_vel, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4),
+            tma::load_3d(base + G::CUR + G::PTW, &m_vel, ti.z0 - (G::H - 4), ti.x0 - (G::H - 4) + sd.vel_col,
                          a.vel_shared ? 0 : ti.s, &full[stg]);
         }
         // never leave copies in flight behind an exiting CTA: wait (bounded)

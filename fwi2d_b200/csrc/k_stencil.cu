@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) fwd_step_kernel(FwdArgs a) {
     const int z0 = blockIdx.x * (4 * kTZ4), x0 = blockIdx.y * kTX;
     const float* cur = a.cur + (size_t)s * a.fstride;
     float* nxt = a.nxt + (size_t)s * a.fstride;
-    const float* vel = a.vel + (size_t)s * a.vel_stride;
+    const float* vel = a.vel + (size_t)s * a.vel_stride + (size_t)sd.vel_col * a.ldz;
 
     // Receivers read Q^t, which this launch never writes.
     if (a.rec_sample >= 0 && blockIdx.x == 0 && blockIdx.y == 0) {
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) fwd_step_kernel(FwdArgs a) {
                 const st::Rows rr = st::rows_info(a.b1d, a.nb, pt % a.ldz, a.nzz);
                 v *= st::damp(rr, st::col_info(a.b1d, a.nb, pt / a.ldz, nxx), 0);
             }
-            a.seis[sd.seis_off + (long long)r * a.nt + a.rec_sample] = v;
+            a.seis[__ldg(a.rec_soff + sd.rec_off + r) + a.rec_sample] = v;
         }
     }
     if (x0 >= nxx) return;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kThreads) bwd_step_kernel(BwdArgs a) {
     const int z0 = blockIdx.x * (4 * kTZ4), x0 = blockIdx.y * kTX;
     if (x0 >= nxx) return;
     const size_t fo = (size_t)s * a.fstride;
-    const float* vel = a.vel + (size_t)s * a.vel_stride;
+    const float* vel = a.vel + (size_t)s * a.vel_stride + (size_t)sd.vel_col * a.ldz;
     float* acc_a = a.acc_a + (size_t)s * a.acc_stride;
     float* acc_b = a.acc_b + (size_t)s * a.acc_stride;
 

@@ -34,16 +34,27 @@ __global__ void expand_kernel(const float* __restrict__ model, int nz, int nx, f
 }
 
 __global__ void crop_sum_kernel(const float* __restrict__ padded, long long stride, int nshots, int nb, int ldz,
-                                int nz, int nx, float* __restrict__ out, bool accumulate) {
+                                int nz, int nx, const int* __restrict__ c0, const int* __restrict__ w,
+                                float* __restrict__ out, bool accumulate) {
     const long long n = (long long)nz * nx;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
          c += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(c / nz), i = (int)(c - (long long)j * nz);
-        const size_t off = (size_t)(j + nb) * ldz + (i + nb);
         float acc = accumulate ? out[c] : 0.0f;
-        for (int s = 0; s < nshots; ++s) acc += padded[(size_t)s * stride + off];
+        for (int s = 0; s < nshots; ++s) {
+            const int lj = j - __ldg(c0 + s);
+            if (lj < 0 || lj >= __ldg(w + s)) continue;
+            acc += padded[(size_t)s * stride + (size_t)(lj + nb) * ldz + (i + nb)];
+        }
         out[c] = acc;
     }
+}
+
+__global__ void mask_traces_kernel(float* __restrict__ data, const unsigned char* __restrict__ keep, size_t ntraces,
+                                   int nt) {
+    const size_t n = ntraces * (size_t)nt;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        if (!keep[c / nt]) data[c] = 0.0f;
 }
 
 __global__ void rtm_post_kernel(const float* __restrict__ img, const float* __restrict__ illum, int nz, int nx,
@@ -154,13 +165,13 @@ __global__ void finite_kernel(const float* __restrict__ x, size_t n, int* flag) 
 
 __global__ void inject_points_kernel(float* field, long long fstride, const ShotDesc* shots, InjTable inj,
                                      int ldz) {
-    const int s = blockIdx.x;
+    const int s = blockIdx.y;
     const ShotDesc sd = shots[s];
     float* f = field + (size_t)s * fstride;
     if (inj.sample < 0) return;
-    // one thread per shot keeps the per-point order of the step kernel
-    if (threadIdx.x != 0) return;
-    for (int j = 0; j < sd.nxx; ++j) {
+    // one thread per column: points of different columns never share a cell,
+    // and a column's points are added in table order as in the step kernel
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < sd.nxx; j += gridDim.x * blockDim.x) {
         const int kb = inj.colptr[sd.col_off + j], ke = inj.colptr[sd.col_off + j + 1];
         for (int k = kb; k < ke; ++k)
             f[(size_t)j * ldz + inj.z[k]] += inj.scale * inj.series[inj.soff[k] + inj.sample];
@@ -182,9 +193,13 @@ void launch_expand(const float* model, int nz, int nx, float* out, long long out
 }
 
 void launch_crop_sum(const float* padded, long long stride, int nshots, int nb, int ldz, int nz, int nx,
-                     float* out, bool accumulate, cudaStream_t st) {
-    crop_sum_kernel<<<grid_for((size_t)nz * nx), 256, 0, st>>>(padded, stride, nshots, nb, ldz, nz, nx, out,
+                     const int* c0, const int* w, float* out, bool accumulate, cudaStream_t st) {
+    crop_sum_kernel<<<grid_for((size_t)nz * nx), 256, 0, st>>>(padded, stride, nshots, nb, ldz, nz, nx, c0, w, out,
                                                                accumulate);
+}
+
+void launch_mask_traces(float* data, const unsigned char* keep, size_t ntraces, int nt, cudaStream_t st) {
+    mask_traces_kernel<<<grid_for(ntraces * (size_t)nt), 256, 0, st>>>(data, keep, ntraces, nt);
 }
 
 void launch_rtm_post(const float* img, const float* illum, int nz, int nx, float idh2, float* out,
@@ -229,7 +244,7 @@ void launch_check_finite(const float* x, size_t n, int* flag, cudaStream_t st) {
 
 void launch_inject_points(float* field, long long fstride, const ShotDesc* shots, int nshots, InjTable inj,
                           int ldz, cudaStream_t st) {
-    inject_points_kernel<<<nshots, 32, 0, st>>>(field, fstride, shots, inj, ldz);
+    inject_points_kernel<<<dim3(8, nshots), 256, 0, st>>>(field, fstride, shots, inj, ldz);
 }
 
 }  // namespace fwi

@@ -21,10 +21,12 @@ constexpr double kFDM5 = 2.847222222222;
 
 struct ShotDesc {
     int nxx;             // padded width (columns) of this shot's grid
-    int nrec;            // receivers of this shot
-    int rec_off;         // first entry of the shot in rec_pt[]
+    int nrec;            // receivers of this shot (those inside its aperture)
+    int rec_off;         // first entry of the shot in rec_pt[] / receiver tables
     int col_off;         // first entry of the shot's injection column table
     long long seis_off;  // float offset of the shot's nt x nrec trace-major block
+    int vel_col;         // column of the velocity array that is column 0 of the
+                         // shot's grid (aperture window over a shared velocity)
 };
 
 // Point injections into the field written by a step (the source of a forward
@@ -52,6 +54,7 @@ struct FwdArgs {
     const float* b1d;         // ABC damping profile (nb floats), NULL for none
     InjTable inj;
     const int* rec_pt;        // receiver points z + x*ldz, per shot at rec_off
+    const long long* rec_soff;// trace offset (into seis) of each rec_pt entry
     float* seis;              // trace-major seismograms
     int rec_sample;           // sample recorded at this step, or -1
     int nt;

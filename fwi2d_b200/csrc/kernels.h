@@ -62,9 +62,12 @@ void launch_rbc(const RbcArgs& a, int nshots, cudaStream_t st);
 // one window per shot (c0[s], w[s]); rows nzz..ldz-1 are zeroed.
 void launch_expand(const float* model, int nz, int nx, float* out, long long out_stride, const int* c0,
                    const int* w, int nshots, int nb, int nzz, int ldz, int max_nxx, cudaStream_t st);
-// out(i,j) = sum over shots of padded(i+nb, j+nb); nz x nx.
+// out(i,x) (+)= sum over the shots s whose window [c0[s], c0[s]+w[s]) holds
+// column x of padded_s(i+nb, x-c0[s]+nb); nz x nx.  Fixed shot order.
 void launch_crop_sum(const float* padded, long long stride, int nshots, int nb, int ldz, int nz, int nx,
-                     float* out, bool accumulate, cudaStream_t st);
+                     const int* c0, const int* w, float* out, bool accumulate, cudaStream_t st);
+// Zeroes the nt samples of every trace whose keep[] entry is 0.
+void launch_mask_traces(float* data, const unsigned char* keep, size_t ntraces, int nt, cudaStream_t st);
 // RTM post-processing (migration.cu:90-115): q = img/illum, out = -d2q/dz2 * idh2.
 void launch_rtm_post(const float* img, const float* illum, int nz, int nx, float idh2, float* out, cudaStream_t st);
 // Gradient post-processing (inversion.cu:136-165) without the final scaling:

@@ -177,6 +177,32 @@ def config2(root, seed: int = 2, **over) -> tuple[Case, np.ndarray]:
     return case, vp
 
 
+def config3(root, seed: int = 3, **over) -> tuple[Case, np.ndarray]:
+    """Batched uneven-aperture FWI: the config-2 model and receiver spread,
+    240 shots every 70 m, each modeled on the columns within its own maximum
+    offset (uniform 1.5-8 km from the seed; windows of about 300-1700 columns)."""
+    nz, nx, dh = 301, 1701, 10.0
+    vp = dipping_model(nz, nx, dh, 2)
+    sx = np.arange(240) * 70.0 + 100.0
+    rx = np.arange(851) * 20.0
+    rng = np.random.default_rng(seed)
+    offsets = rng.uniform(1500.0, 8000.0, sx.size).astype(np.float32)
+    kw = dict(nt=4001, dt=1e-3, fmax=15.0)
+    kw.update({k: over.pop(k) for k in list(over) if k in kw})
+    root = Path(root)
+    root.mkdir(parents=True, exist_ok=True)
+    write_offsets(root / "offsets.txt", offsets)
+    over.setdefault("aperture_file", f"{root}/offsets.txt")
+    case = write_case(root, vp, dh, kw["nt"], kw["dt"], kw["fmax"], sx, np.full(sx.size, 10.0), rx,
+                      np.full(851, 10.0), **over)
+    return case, vp
+
+
+def write_offsets(path, offsets) -> None:
+    """One maximum offset (metres) per shot, as the key aperture_file reads them."""
+    Path(path).write_text("".join(f"{float(np.float32(o)):.6g}\n" for o in offsets))
+
+
 def small_case(root, seed: int = 5, nz: int = 48, nx: int = 96, dh: float = 10.0, nt: int = 500, fmax: float = 30.0,
                nshots: int = 3, nrec: int = 24, boundary: float = 190.0, **over) -> tuple[Case, np.ndarray]:
     """A few-second case for parity tests: layered model, `nshots` shots and
@@ -187,6 +213,12 @@ def small_case(root, seed: int = 5, nz: int = 48, nx: int = 96, dh: float = 10.0
     rx = np.linspace(0.0, w, nrec)
     keys = dict(abc_length=boundary, inv_rbc_length=boundary, mig_rbc_length=boundary, inv_rbc_ratio=60,
                 mig_rbc_ratio=60, max_iteration=2)
+    offsets = keys.pop("max_offsets", None)
     keys.update(over)
+    offsets = keys.pop("max_offsets", offsets)
+    if offsets is not None:
+        Path(root).mkdir(parents=True, exist_ok=True)
+        write_offsets(Path(root) / "offsets.txt", offsets)
+        keys["aperture_file"] = f"{root}/offsets.txt"
     case = write_case(root, vp, dh, nt, 1e-3, fmax, sx, np.full(nshots, 20.0), rx, np.full(nrec, 10.0), **keys)
     return case, vp

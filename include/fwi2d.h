@@ -79,7 +79,8 @@ int  fwi_get_stream(const fwi_ctx* ctx, void** stream);
 /* Value of a parameters.txt key under the reference's rules (admin.cpp:53-98);
  * FWI_ERR_PARAM when absent, FWI_ERR_ARG when buf (len bytes) is too small. */
 int  fwi_get_param(const fwi_ctx* ctx, const char* key, char* buf, size_t len);
-/* Seed of the random-boundary generator (default from key rbc_seed, else 0). */
+/* Seed of the random-boundary generator (default from key rbc_seed, else 0);
+ * restarts the sequence of per-gradient-pass boundaries. */
 int  fwi_set_seed(fwi_ctx* ctx, uint64_t seed);
 
 /* Velocity model, nz x nx.  Replaces set_properties/expand_boundary
@@ -91,6 +92,14 @@ int  fwi_get_wavelet(fwi_ctx* ctx, float* w);
 /* Grid indices of shot `shot`: sIdx,sIdz (2 ints) and rIdx[nrec], rIdz[nrec];
  * initialization, modeling.cu:252-277.  Any pointer may be NULL. */
 int  fwi_get_indices(fwi_ctx* ctx, int shot, int* src_xz, int* rec_x, int* rec_z);
+/* Aperture window of shot `shot`: model columns [*c0, *c0 + *w).  The whole
+ * model (0, nx) unless the parameter file sets aperture_offset (maximum
+ * offset in metres, every shot) or aperture_file (a text file with one maximum
+ * offset per shot).  A windowed shot is modeled on its
+ * window padded by the boundary; receivers outside it record nothing and, in
+ * an inversion, their traces take no part in the misfit.  No reference
+ * counterpart: the reference models every shot on the whole model. */
+int  fwi_get_window(fwi_ctx* ctx, int shot, int* c0, int* w);
 
 /* ---- modeling ------------------------------------------------------------
  * One shot: initialization + forward_solver + get_seismogram without the file
@@ -124,6 +133,27 @@ int  fwi_set_observed_dev(fwi_ctx* ctx, const float* d_obs_all);
  * FP64 misfit, and - when with_gradient != 0 - RBC forward + adjoint back-
  * propagation + gradient post-processing.  *sum_res = sum of residual^2. */
 int  fwi_compute_gradient(fwi_ctx* ctx, int with_gradient, double* sum_res);
+/* ---- sharded inversion (shots split over processes / GPUs) ---------------
+ * fwi_compute_gradient(ctx, 1, s) equals fwi_gradient_accumulate followed by
+ * fwi_gradient_finish.  A process that owns shots [s0, s0+ns) sets its range,
+ * accumulates, sums the two raw accumulators (and the misfit) over all
+ * processes in place - e.g. an NCCL all-reduce on the device buffers that
+ * fwi_accumulators returns - and then finishes; fwi_linesearch_trial sums over
+ * the range too, and fwi_parabola_step turns the summed misfits into the step
+ * of optimization (inversion.cu:286-308).  The range (default: all shots)
+ * applies to fwi_compute_gradient, fwi_gradient_accumulate and
+ * fwi_linesearch_trial. */
+int  fwi_set_shot_range(fwi_ctx* ctx, int s0, int ns);
+int  fwi_gradient_accumulate(fwi_ctx* ctx, int with_gradient, double* sum_res);
+int  fwi_gradient_finish(fwi_ctx* ctx);
+/* Device pointers (nz x nx floats each, owned by the context) of the raw
+ * cross-correlation (RTM image or FWI gradient) and source-illumination
+ * accumulators; the context's stream is idle when the call returns. */
+int  fwi_accumulators(fwi_ctx* ctx, float** d_image_or_gradient, float** d_illum);
+/* Trial steps a1 = 0.02 dm, a2 = 0.05 dm of the current model and the
+ * parabola vertex of misfits f0, f1, f2 at 0, a1, a2 (inversion.cu:286-308). */
+int  fwi_trial_steps(fwi_ctx* ctx, float* a1, float* a2);
+int  fwi_parabola_step(fwi_ctx* ctx, float f0, float f1, float f2, float* step);
 /* Post-processed gradient (nz x nx, normalised by max |g|) */
 int  fwi_get_gradient(fwi_ctx* ctx, float* g);
 /* Raw gradient and illumination (nz x nx, cropped, before post-processing). */
@@ -140,7 +170,8 @@ int  fwi_update_model(fwi_ctx* ctx, float step, float* vp_out);
 
 /* ---- random boundary ----------------------------------------------------
  * set_random_boundary (modeling.cu:431-531) for shot `shot` of the current
- * model, on the context's RBC grid; out is nzz x nxx (z fastest, unpitched). */
+ * model, on the context's RBC grid; out is nzz x (w + 2 nb) (z fastest,
+ * unpitched), w the shot's window width (nx without windows). */
 int  fwi_random_boundary(fwi_ctx* ctx, int shot, float* vp_rbc);
 
 /* ---- host-side utilities (no GPU, no context) -----------------------------
@@ -154,6 +185,10 @@ int  fwi_util_wavelet(int nt, float dt, float fmax, float* out, int* tlag);
 int  fwi_util_b1d(int nb, float abc_factor, float* out);
 /* initialization's index rule int((c + dh/2)/dh) + nb (modeling.cu:257-269). */
 int  fwi_util_grid_index(int n, const float* coord, float dh, int nb, int* out);
+/* Aperture window of a source at x = xs (metres) for a maximum offset
+ * max_offset: model columns [*c0, *c0 + *w) of an nx-column model (the rule of
+ * fwi_get_window; no reference counterpart). */
+int  fwi_util_window(float xs, float max_offset, int nx, float dh, int* c0, int* w);
 /* Random-boundary bumps of one shot (modeling.cu:431-465): 5 floats
  * (xc, zc, r, A, sign) per bump; *count = bumps generated (may exceed cap). */
 int  fwi_util_bumps(int nxx, int nzz, int nb, float dh, float ratio, float varVp, uint64_t seed,
@@ -183,6 +218,15 @@ int  fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, 
 int  fwi_describe(fwi_ctx* ctx, char* buf, size_t len);
 /* Kernel launches issued by the context since creation (or the last reset). */
 int  fwi_launch_count(fwi_ctx* ctx, long long* count, int reset);
+/* Forward-kernel timing.  fwi_fwd_timing(ctx, 1) resets the counters and
+   brackets every later launch of the forward propagation kernel (a
+   multi-level launch, or the graph of one-level launches of a batch) with
+   CUDA events on the context stream; 0 turns it off.  fwi_fwd_timing_read
+   waits for the recorded events and returns the summed device time in ms,
+   the number of forward-kernel launches covered and the grid-point updates
+   they performed (padded points x time levels x shots). */
+int  fwi_fwd_timing(fwi_ctx* ctx, int enable);
+int  fwi_fwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates);
 
 #ifdef __cplusplus
 }

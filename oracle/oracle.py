@@ -130,6 +130,43 @@ def crop(padded: np.ndarray, nb: int) -> np.ndarray:
     return padded[nb:padded.shape[0] - nb, nb:padded.shape[1] - nb]
 
 
+# ------------------------------------------------- aperture windows (extension)
+# Batched uneven-aperture surveys have no reference counterpart: the reference
+# models every shot on the whole model.  These restate the engine's rule from
+# its definition so the windowed paths have a CPU check.
+def window(xs: float, max_offset: float, nx: int, dh: float) -> tuple[int, int]:
+    """Model columns [c0, c0+w) within max_offset of a source at x = xs."""
+    import math
+    c0 = math.floor((float(xs) - float(max_offset)) / float(dh))
+    c1 = math.ceil((float(xs) + float(max_offset)) / float(dh))
+    c0 = min(max(c0, 0), nx - 1)
+    c1 = min(max(c1, 0), nx - 1)
+    while c1 - c0 + 1 < 9:
+        if c0 > 0:
+            c0 -= 1
+        if c1 - c0 + 1 < 9 and c1 < nx - 1:
+            c1 += 1
+    return c0, c1 - c0 + 1
+
+
+def window_velocity_abc(model: np.ndarray, nb: int, c0: int, w: int) -> np.ndarray:
+    """ABC grid of a windowed shot: columns c0 .. c0+w+2nb-1 of the padded whole model."""
+    return expand(model, nb)[:, c0:c0 + w + 2 * nb]
+
+
+def window_velocity_rbc_base(model: np.ndarray, nb: int, c0: int, w: int) -> np.ndarray:
+    """RBC base of a windowed shot: its window padded by edge replication."""
+    return expand(np.ascontiguousarray(model[:, c0:c0 + w]), nb)
+
+
+def scatter_windows(parts, windows, nz: int, nx: int, nb: int) -> np.ndarray:
+    """Sum over shots of crop(part_s) placed at columns [c0_s, c0_s + w_s)."""
+    out = np.zeros((nz, nx), np.float64)
+    for p, (c0, w) in zip(parts, windows):
+        out[:, c0:c0 + w] += crop(p, nb)
+    return out
+
+
 # --------------------------------------------------------------- propagation
 def forward(vel: np.ndarray, nb: int, b1d_tab, wav: np.ndarray, nt: int, tlag: int, dt: float, dh: float,
             src: tuple[int, int], rx, rz, bits: int = 64, ordered: bool = False):
