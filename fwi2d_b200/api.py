@@ -56,6 +56,9 @@ SIGNATURES = {
     "fwi_get_wavelet": (C.c_int, [_P, _F]),
     "fwi_get_indices": (C.c_int, [_P, C.c_int, _I, _I, _I]),
     "fwi_get_window": (C.c_int, [_P, C.c_int, _I, _I]),
+    "fwi_mute_direct": (C.c_int, [_P, _F, C.c_float, C.c_float, C.c_float]),
+    "fwi_mute_direct_dev": (C.c_int, [_P, C.c_void_p, C.c_float, C.c_float, C.c_float]),
+    "fwi_smooth_model": (C.c_int, [_P, _F, C.c_float, C.c_float, _F]),
     "fwi_set_shot_range": (C.c_int, [_P, C.c_int, C.c_int]),
     "fwi_gradient_accumulate": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double)]),
     "fwi_gradient_finish": (C.c_int, [_P]),
@@ -93,6 +96,7 @@ SIGNATURES = {
     "fwi_describe": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fwi_fwd_timing": (C.c_int, [_P, C.c_int]),
     "fwi_fwd_timing_read": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "fwi_bwd_timing_read": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 
@@ -190,6 +194,12 @@ class Context:
         """(device ms, forward-kernel launches, grid-point updates) since fwd_timing(True)."""
         ms, n, u = C.c_double(), C.c_longlong(), C.c_longlong()
         self._check(self._lib.fwi_fwd_timing_read(self._h, C.byref(ms), C.byref(n), C.byref(u)))
+        return ms.value, n.value, u.value
+
+    def bwd_timing_read(self) -> tuple[float, int, int]:
+        """(device ms, backward-kernel launches, grid-point updates) since fwd_timing(True)."""
+        ms, n, u = C.c_double(), C.c_longlong(), C.c_longlong()
+        self._check(self._lib.fwi_bwd_timing_read(self._h, C.byref(ms), C.byref(n), C.byref(u)))
         return ms.value, n.value, u.value
 
     def launches(self, reset: bool = False) -> int:
@@ -363,6 +373,21 @@ class Context:
     def update_model(self, step: float) -> np.ndarray:
         out = self._grid_out()
         self._check(self._lib.fwi_update_model(self._h, step, _fptr(out)))
+        return self._as2d(out)
+
+    # -- data preparation (run/generate_input_data.py, run/generate_setup.py)
+    def mute_direct(self, data: np.ndarray, velocity: float = 3600.0, delay: float = 0.18,
+                    gstd: float = 30.0) -> np.ndarray:
+        """Muted copy of (nsrc, nt, nrec) seismograms."""
+        flat = self._traces(data).copy()
+        self._check(self._lib.fwi_mute_direct(self._h, _fptr(flat), velocity, delay, gstd))
+        d = self.dims
+        return flat.reshape(d.nsrc, d.nrec, d.nt).transpose(0, 2, 1)
+
+    def smooth_model(self, vp: np.ndarray, sigma: float = 3.0, depth_mask: float = 0.0) -> np.ndarray:
+        src = np.ascontiguousarray(np.asarray(vp, dtype=np.float32).T).ravel()
+        out = self._grid_out()
+        self._check(self._lib.fwi_smooth_model(self._h, _fptr(src), sigma, depth_mask, _fptr(out)))
         return self._as2d(out)
 
     def random_boundary(self, shot: int) -> np.ndarray:

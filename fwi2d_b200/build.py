@@ -35,6 +35,8 @@ CU_SOURCES = {
     "k_stencil.cu": [],
     "k_fwd_tma.cu": [],
     "k_fwd_loop.cu": [],
+    "k_bwd_loop.cu": [],
+    "k_prep.cu": ["-fmad=false"],
     "k_util.cu": [],
     "k_rbc.cu": ["-fmad=false"],
     "k_noalloc.cu": [],

@@ -257,6 +257,18 @@ int fwi_update_model(fwi_ctx* ctx, float step, float* vp_out) {
     return guarded(ctx, [&](fwi::Engine& e) { e.update_model(step, vp_out); });
 }
 
+int fwi_mute_direct(fwi_ctx* ctx, float* data_all, float velocity, float delay, float gstd) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.mute_direct(data_all, false, velocity, delay, gstd); });
+}
+
+int fwi_mute_direct_dev(fwi_ctx* ctx, float* d_data_all, float velocity, float delay, float gstd) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.mute_direct(d_data_all, true, velocity, delay, gstd); });
+}
+
+int fwi_smooth_model(fwi_ctx* ctx, const float* vp, float sigma, float depth_mask, float* vp_out) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.smooth_model(vp, sigma, depth_mask, vp_out); });
+}
+
 int fwi_random_boundary(fwi_ctx* ctx, int shot, float* vp_rbc) {
     if (!vp_rbc) return arg_error(ctx, "NULL output");
     return guarded(ctx, [&](fwi::Engine& e) { e.random_boundary(shot, vp_rbc); });
@@ -347,7 +359,8 @@ int fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, s
 
 int fwi_describe(fwi_ctx* ctx, char* buf, size_t len) {
     if (!ctx || !ctx->eng || !buf || len == 0) return FWI_ERR_ARG;
-    const std::string& s = ctx->eng->last_fwd_plan;
+    std::string s = ctx->eng->last_fwd_plan;
+    if (!ctx->eng->last_bwd_plan.empty()) s += " || backward: " + ctx->eng->last_bwd_plan;
     if (s.size() + 1 > len) return FWI_ERR_ARG;
     std::memcpy(buf, s.c_str(), s.size() + 1);
     return FWI_OK;
@@ -365,6 +378,11 @@ int fwi_fwd_timing(fwi_ctx* ctx, int enable) {
 int fwi_fwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates) {
     if (!ms || !launches || !updates) return arg_error(ctx, "NULL output");
     return guarded(ctx, [&](fwi::Engine& e) { e.fwd_timing_read(ms, launches, updates); });
+}
+
+int fwi_bwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates) {
+    if (!ms || !launches || !updates) return arg_error(ctx, "NULL output");
+    return guarded(ctx, [&](fwi::Engine& e) { e.bwd_timing_read(ms, launches, updates); });
 }
 
 }  // extern "C"

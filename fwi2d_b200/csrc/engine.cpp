@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <numeric>
 #include <sstream>
 #include <type_traits>
@@ -74,6 +75,8 @@ Engine::Engine(const std::string& params_path, int mode) : P_(params_path), mode
     use_graphs_ = std::getenv("FWI2D_NO_GRAPHS") == nullptr;
     fwd_kernel_ = P_.str_or("fwd_kernel", "auto");
     if (const char* e = std::getenv("FWI2D_FWD_KERNEL")) fwd_kernel_ = e;
+    bwd_kernel_ = P_.str_or("bwd_kernel", "auto");
+    if (const char* e = std::getenv("FWI2D_BWD_KERNEL")) bwd_kernel_ = e;
 
     wavelet_ = make_wavelet(nt_, dt_, fmax_, &tlag_);
     geo_ = read_geometry(P_.str("SPS"), P_.str("RPS"));
@@ -289,6 +292,17 @@ void Engine::alloc_buffers() {
         w[s] = win_[s].w;
         nxx[s] = has_rbc_ ? rbc_t_.nxx[s] : abc_t_.nxx[s];
     }
+    {
+        std::vector<float> geo;
+        geo.insert(geo.end(), geo_.xsrc.begin(), geo_.xsrc.end());
+        geo.insert(geo.end(), geo_.zsrc.begin(), geo_.zsrc.end());
+        geo.insert(geo.end(), geo_.xrec.begin(), geo_.xrec.end());
+        geo.insert(geo.end(), geo_.zrec.begin(), geo_.zrec.end());
+        d_geo_ = dalloc<float>(geo.size(), "geometry");
+        check(cudaMemcpy(d_geo_, geo.data(), geo.size() * sizeof(float), cudaMemcpyHostToDevice), "upload geometry");
+        d_shot_bits_ = dalloc<unsigned>(nsrc_, "per-shot scratch");
+        d_weights_ = dalloc<double>(1024, "filter weights");
+    }
     const int full[2] = {0, nx_};
     d_full_win_ = dalloc<int>(2, "whole-model window");
     check(cudaMemcpy(d_full_win_, full, sizeof(full), cudaMemcpyHostToDevice), "upload whole-model window");
@@ -319,7 +333,7 @@ Engine::~Engine() {
                     d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
                     d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_, d_sync_,
-                    d_full_win_, d_trace_keep_};
+                    d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& r : timed_) {
@@ -335,8 +349,8 @@ void Engine::fwd_timing(bool enable) {
     double ms;
     long long l, u;
     fwd_timing_read(&ms, &l, &u);  // drain recorded regions
-    timed_ms_ = 0;
-    timed_launches_ = timed_updates_ = 0;
+    timed_ms_ = btimed_ms_ = 0;
+    timed_launches_ = timed_updates_ = btimed_launches_ = btimed_updates_ = 0;
     timing_ = enable;
 }
 
@@ -371,9 +385,15 @@ void Engine::fwd_timing_read(double* ms, long long* launches, long long* updates
         check(cudaEventSynchronize(r.end), "timing event");
         float t = 0.f;
         check(cudaEventElapsedTime(&t, r.begin, r.end), "timing elapsed");
-        timed_ms_ += t;
-        timed_launches_ += r.launches;
-        timed_updates_ += r.updates;
+        if (r.launches >= 0) {
+            timed_ms_ += t;
+            timed_launches_ += r.launches;
+            timed_updates_ += r.updates;
+        } else {  // a backward region
+            btimed_ms_ += t;
+            btimed_launches_ -= r.launches;
+            btimed_updates_ += r.updates;
+        }
         event_pool_.push_back(r.begin);
         event_pool_.push_back(r.end);
     }
@@ -381,6 +401,13 @@ void Engine::fwd_timing_read(double* ms, long long* launches, long long* updates
     *ms = timed_ms_;
     *launches = timed_launches_;
     *updates = timed_updates_;
+}
+
+void Engine::bwd_timing_read(double* ms, long long* launches, long long* updates) {
+    fwd_timing_read(ms, launches, updates);
+    *ms = btimed_ms_;
+    *launches = btimed_launches_;
+    *updates = btimed_updates_;
 }
 
 fwi_dims Engine::dims() const {
@@ -967,6 +994,162 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     check(cudaGetLastError(), "forward propagation");
 }
 
+Engine::BwdPlan Engine::bwd_plan(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride,
+                                 bool gradient, const float* d_series, float* scratch0, float* scratch1) {
+    const long long key = (((long long)(&g == &abc_ ? 0 : 1) * 2 + (gradient ? 1 : 0)) * 2 + (vel_stride ? 1 : 0)) *
+                              1000000LL + ns;
+    auto it = bwd_plans_.find(key);
+    if (it != bwd_plans_.end()) return it->second;
+    auto make_loop = [&](int TX, int S) {
+        BwdPlan p;
+        p.kind = 2;
+        p.TX = TX;
+        p.S = S;
+        int ctas = 0;
+        if (bwd_loop_configure(&ctas, TX, S) != cudaSuccess || ctas < 1) {
+            cudaGetLastError();
+            p.kind = -1;
+            return p;
+        }
+        p.grid = sm_count_ * ctas;
+        return p;
+    };
+    std::vector<BwdPlan> cands;
+    if (bwd_kernel_ == "simple") {
+        cands.push_back(BwdPlan{});
+    } else if (bwd_kernel_.rfind("loop:", 0) == 0) {
+        int TX = 0, S = 0;
+        if (std::sscanf(bwd_kernel_.c_str() + 5, "%d,%d", &TX, &S) != 2 || !bwd_loop_supported(TX, S))
+            throw Error(FWI_ERR_PARAM, "bwd_kernel '" + bwd_kernel_ + "' is not a compiled multi-level variant");
+        cands.push_back(make_loop(TX, S));
+    } else if (bwd_kernel_ == "auto") {
+        cands.push_back(BwdPlan{});
+        const int loops[][2] = {{16, 3}, {16, 2}, {8, 4}, {8, 3}};
+        for (const auto& v : loops) cands.push_back(make_loop(v[0], v[1]));
+    } else {
+        throw Error(FWI_ERR_PARAM, "bwd_kernel must be auto, simple or loop:TX,S");
+    }
+    // Candidates run on scratch buffers only (the forward's final fields stay
+    // untouched): both fields alias scratch0/scratch1, the accumulators are
+    // cleared by the caller afterwards.
+    BwdPlan best;
+    double best_us = 1e30;
+    std::ostringstream log;
+    const int levels = 24;
+    float* ps[2] = {scratch0, scratch1};
+    float* pr[2] = {scratch1, scratch0};
+    const dim3 grid = step_grid(g.ldz, g.nxx, ns);
+    for (auto& c : cands) {
+        if (c.kind < 0) continue;
+        if (cands.size() == 1) {
+            best = c;
+            break;
+        }
+        auto run = [&](int nlev) {
+            if (c.kind == 2) {
+                upload_tile_base(g, ns, c.TX);
+                launch_bwd_loop_levels(c, g, t, ns, vel, vel_stride, gradient, d_series, ps, pr, 0, nlev);
+                return;
+            }
+            for (int b = 0; b < nlev; ++b) {
+                BwdArgs a;
+                a.shots = d_batch_;
+                a.vel = vel;
+                a.vel_stride = vel_stride;
+                a.ps_st = ps[(b + 1) & 1];
+                a.ps_io = ps[b & 1];
+                a.pr_st = pr[b & 1];
+                a.pr_io = pr[(b + 1) & 1];
+                a.fstride = g.fstride();
+                a.acc_a = acc_[0];
+                a.acc_b = acc_[1];
+                a.acc_stride = g.fstride();
+                a.ldz = g.ldz;
+                a.nzz = g.nzz;
+                a.dt2idh2 = dt_ * dt_ * idh2_;
+                a.dt = dt_;
+                a.idh2 = idh2_;
+                a.inj = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, d_series, nt_ - 2 - b, idh2_};
+                if (a.inj.sample < 0) a.inj.sample = -1;
+                launch_bwd_step(a, gradient, grid, st_);
+            }
+        };
+        run(2);  // first use
+        cudaEvent_t e0, e1;
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            check(cudaEventRecord(e0, st_), "event record");
+            run(levels);
+            check(cudaEventRecord(e1, st_), "event record");
+            check(cudaEventSynchronize(e1), "event sync");
+            float m = 0.f;
+            cudaEventElapsedTime(&m, e0, e1);
+            ms = std::min(ms, m);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c.us_per_step = 1e3 * ms / levels;
+        if (c.kind == 0) log << " simple=" << c.us_per_step;
+        else log << " loop" << c.TX << "," << c.S << "=" << c.us_per_step;
+        if (c.us_per_step < best_us) {
+            best_us = c.us_per_step;
+            best = c;
+        }
+    }
+    sync("backward autotune");
+    best.tuning = log.str();
+    bwd_plans_[key] = best;
+    return best;
+}
+
+void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                                    long long vel_stride, bool gradient, const float* d_series, float* const ps[2],
+                                    float* const pr[2], int b_begin, int b_end, long long timed_updates) {
+    const int R = fwd_tma_rows();
+    BwdLoopMaps maps;
+    for (int q = 0; q < 2; ++q) {
+        maps.ps_st[q] = tmap(ps[q ^ 1], g, batch_, R + 8, p.TX + 8);
+        maps.pr_st[q] = tmap(pr[q], g, batch_, R + 8, p.TX + 8);
+        maps.ps_pt[q] = tmap(ps[q], g, batch_, R, p.TX);
+        maps.pr_pt[q] = tmap(pr[q ^ 1], g, batch_, R, p.TX);
+    }
+    maps.acc_a = tmap(acc_[0], g, batch_, R, p.TX);
+    maps.acc_b = tmap(acc_[1], g, batch_, R, p.TX);
+    maps.vel = tmap(vel, g, vel_stride ? batch_ : 1, R, p.TX, vel_stride == 0);
+    BwdLoopArgs a;
+    a.shots = d_batch_;
+    a.tile_base = d_tile_base_;
+    a.ns = ns;
+    a.ntz = (g.ldz + R - 1) / R;
+    a.ldz = g.ldz;
+    a.nzz = g.nzz;
+    a.fstride = g.fstride();
+    a.vel_shared = vel_stride == 0 ? 1 : 0;
+    a.dt2idh2 = dt_ * dt_ * idh2_;
+    a.dt = dt_;
+    a.idh2 = idh2_;
+    a.inj = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, d_series, -1, idh2_};
+    a.nt = nt_;
+    a.b_begin = b_begin;
+    a.b_end = b_end;
+    a.ps[0] = ps[0];
+    a.ps[1] = ps[1];
+    a.pr[0] = pr[0];
+    a.pr[1] = pr[1];
+    a.acc_a = acc_[0];
+    a.acc_b = acc_[1];
+    a.err = d_err_;
+    a.sync = d_sync_;
+    check(cudaMemsetAsync(d_sync_, 0, sizeof(unsigned), st_), "memset grid barrier");
+    TimedRegion r;
+    if (timed_updates >= 0) timing_begin(&r);
+    check(launch_bwd_loop(p.TX, p.S, gradient, maps, a, p.grid, st_), "multi-level backward launch");
+    if (timed_updates >= 0) timing_end(&r, -1, timed_updates);
+    ++launches_;
+}
+
 void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride,
                           bool gradient, const float* d_series) {
     const long long fs = g.fstride();
@@ -979,6 +1162,14 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
         if (b != X && b != Y && nf < 2) free_buf[nf++] = b;
     float* R0 = free_buf[0];
     float* R1 = free_buf[1];
+    const BwdPlan plan = bwd_plan(g, t, ns, vel, vel_stride, gradient, d_series, R0, R1);
+    {
+        std::ostringstream d;
+        if (plan.kind == 2) d << "loop TX=" << plan.TX << " S=" << plan.S << " grid=" << plan.grid;
+        else d << "simple";
+        if (!plan.tuning.empty()) d << " | us/step:" << plan.tuning;
+        last_bwd_plan = d.str();
+    }
     const size_t bytes = (size_t)ns * fs * sizeof(float);
     check(cudaMemsetAsync(R0, 0, bytes, st_), "memset Pr");
     check(cudaMemsetAsync(R1, 0, bytes, st_), "memset Prold");
@@ -987,6 +1178,15 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
     InjTable inj{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, d_series, nt_ - 1, idh2_};
     launch_inject_points(R0, fs, d_batch_, ns, inj, g.ldz, st_);
     ++launches_;
+    if (plan.kind == 2) {
+        upload_tile_base(g, ns, plan.TX);
+        float* ps[2] = {X, Y};
+        float* pr[2] = {R0, R1};
+        launch_bwd_loop_levels(plan, g, t, ns, vel, vel_stride, gradient, d_series, ps, pr, 0, N,
+                               (long long)N * batch_points(g, ns));
+        check(cudaGetLastError(), "backward propagation");
+        return;
+    }
     const dim3 grid = step_grid(g.ldz, g.nxx, ns);
     const float dt2idh2 = dt_ * dt_ * idh2_;
     auto body = [&]() {
@@ -1021,6 +1221,7 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
     const long long key =
         (((long long)(gradient ? kBwdGradient : kBwdImage) * 8 + 4 + (&g == &abc_ ? 0 : 1)) * 16 + xi * 4 + yi) *
             1000000LL + ns;
+    TimedRegion r;
     if (use_graphs_) {
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
@@ -1033,10 +1234,13 @@ void Engine::run_backward(const Grid& g, const Tables& t, int ns, const float* v
             cudaGraphDestroy(graph);
             it = graphs_.emplace(key, exec).first;
         }
+        timing_begin(&r);
         check(cudaGraphLaunch(it->second, st_), "graph launch");
     } else {
+        timing_begin(&r);
         body();
     }
+    timing_end(&r, -(long long)N, (long long)N * batch_points(g, ns));
     launches_ += N;
     check(cudaGetLastError(), "backward propagation");
 }
@@ -1124,6 +1328,63 @@ void Engine::rtm_raw(float* img, float* illum) {
     if (img) check(cudaMemcpyAsync(img, d_img_, n, cudaMemcpyDeviceToHost, st_), "copy image");
     if (illum) check(cudaMemcpyAsync(illum, d_illum_, n, cudaMemcpyDeviceToHost, st_), "copy illumination");
     sync("rtm_raw");
+}
+
+// ---------------------------------------------------------- data preparation
+void Engine::mute_direct(float* data, bool on_device, float velocity, float delay, float gstd) {
+    if (!data) throw Error(FWI_ERR_ARG, "NULL data");
+    if (!(velocity > 0) || !(dt_ > 0) || !(gstd > 0)) throw Error(FWI_ERR_ARG, "velocity and gstd must be positive");
+    const size_t n = (size_t)nsrc_ * nrec_ * nt_;
+    float* d = data;
+    if (!on_device) {
+        d = d_seis_;
+        check(cudaMemcpyAsync(d, data, n * sizeof(float), cudaMemcpyHostToDevice, st_), "upload data");
+    }
+    launch_mute_direct(d, nsrc_, nrec_, nt_, d_geo_, d_geo_ + nsrc_, d_geo_ + 2 * nsrc_, d_geo_ + 2 * nsrc_ + nrec_,
+                       velocity, delay, dt_, gstd, d_shot_bits_, st_);
+    launches_ += 2;
+    if (!on_device) check(cudaMemcpyAsync(data, d, n * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy data");
+    sync("mute_direct");
+}
+
+void Engine::smooth_model(const float* vp, float sigma, float depth_mask, float* out) {
+    if (!vp || !out) throw Error(FWI_ERR_ARG, "NULL model");
+    if (!(sigma > 0)) throw Error(FWI_ERR_ARG, "sigma must be positive");
+    // scipy.ndimage gaussian_filter1d kernel: radius int(4 sigma + 0.5),
+    // exp(-0.5 x^2 / sigma^2) normalised by its numpy (pairwise) sum
+    const double sd = sigma;
+    const int radius = (int)(4.0 * sd + 0.5);
+    if (radius >= 1024) throw Error(FWI_ERR_ARG, "sigma too large");
+    std::vector<double> phi(2 * radius + 1);
+    for (int k = -radius; k <= radius; ++k) phi[k + radius] = std::exp(-0.5 / (sd * sd) * (double)k * (double)k);
+    double sum;
+    const size_t m = phi.size();
+    if (m < 8) {
+        sum = 0.0;
+        for (double x : phi) sum += x;
+    } else {  // numpy's pairwise_sum for n <= 128: 8 partial sums, then the tail
+        double r[8];
+        for (int j = 0; j < 8; ++j) r[j] = phi[j];
+        size_t i = 8;
+        for (; i < m - m % 8; i += 8)
+            for (int j = 0; j < 8; ++j) r[j] += phi[i + j];
+        sum = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < m; ++i) sum += phi[i];
+    }
+    std::vector<double> half(radius + 1);
+    for (int k = 0; k <= radius; ++k) half[k] = phi[radius + k] / sum;
+    const size_t n = (size_t)nx_ * nz_;
+    const int keep = std::max(0, (int)((double)depth_mask / (double)dh_));
+    // scratch for the input, the z-pass and the result (freed on every exit)
+    std::unique_ptr<float, decltype(&cudaFree)> buf(dalloc<float>(3 * n, "smoothing scratch"), &cudaFree);
+    float* d_in = buf.get();
+    check(cudaMemcpyAsync(d_weights_, half.data(), half.size() * sizeof(double), cudaMemcpyHostToDevice, st_),
+          "upload weights");
+    check(cudaMemcpyAsync(d_in, vp, n * sizeof(float), cudaMemcpyHostToDevice, st_), "upload model");
+    launch_smooth_slowness(d_in, nz_, nx_, d_weights_, radius, keep, d_in + n, d_in + 2 * n, st_);
+    launches_ += 3;
+    check(cudaMemcpyAsync(out, d_in + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy model");
+    sync("smooth_model");
 }
 
 void Engine::random_boundary(int shot, float* out) {

@@ -40,6 +40,7 @@ public:
     // forward-kernel timing (events around each forward propagation launch)
     void fwd_timing(bool enable);
     void fwd_timing_read(double* ms, long long* launches, long long* updates);
+    void bwd_timing_read(double* ms, long long* launches, long long* updates);
 
     void set_model(const float* vp_host);          // nz x nx
     void get_model(float* vp_host);
@@ -75,6 +76,9 @@ public:
     double linesearch_trial(float alpha);
     float optimization(float f0);
     void update_model(float step, float* vp_out);
+    // data preparation (run/generate_input_data.py:22-44, run/generate_setup.py:49-51)
+    void mute_direct(float* data_all, bool on_device, float velocity, float delay, float gstd);
+    void smooth_model(const float* vp_host, float sigma, float depth_mask, float* out_host);
     // random boundary of one shot on the RBC grid, nzz x nxx unpitched
     void random_boundary(int shot, float* out_host);
 
@@ -147,6 +151,19 @@ private:
                              bool record, float* d_seis);
     double time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                               long long vel_stride, bool abc);
+    // backward-kernel choice: the one-level kernel of k_stencil.cu (kind 0) or
+    // a cooperative multi-level variant of k_bwd_loop.cu (kind 2), autotuned
+    struct BwdPlan {
+        int kind = 0;
+        int TX = 16, S = 3, grid = 0;
+        double us_per_step = 0;
+        std::string tuning;
+    };
+    BwdPlan bwd_plan(const Grid& g, const Tables& t, int ns, const float* vel, long long vel_stride, bool gradient,
+                     const float* d_series, float* scratch0, float* scratch1);
+    void launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
+                                long long vel_stride, bool gradient, const float* d_series, float* const ps[2],
+                                float* const pr[2], int b_begin, int b_end, long long timed_updates = -1);
     void launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                                 long long vel_stride, bool abc, bool record, float* d_seis, int t_begin, int t_end,
                                 long long timed_updates = -1);
@@ -196,6 +213,9 @@ private:
     std::vector<Window> win_;
     bool windowed_ = false;
     int* d_full_win_ = nullptr;          // {0} and {nx}: the whole-model window
+    float* d_geo_ = nullptr;             // sx, sz (nsrc each), rx, rz (nrec each)
+    unsigned* d_shot_bits_ = nullptr;    // nsrc scratch words
+    double* d_weights_ = nullptr;        // Gaussian half-kernel (up to 1024 taps)
     unsigned char* d_trace_keep_ = nullptr;  // per trace: receiver inside the shot's window
     // batch being propagated (tables and first survey shot)
     const Tables* batch_t_ = nullptr;
@@ -244,6 +264,8 @@ private:
     // TMA forward path
     std::map<std::string, CUtensorMap> tmaps_;
     std::map<long long, FwdPlan> plans_;
+    std::map<long long, BwdPlan> bwd_plans_;
+    std::string bwd_kernel_ = "auto";  // key bwd_kernel: auto | simple | loop:TX,S
     int* d_tile_base_ = nullptr;
     int* d_err_ = nullptr;
     unsigned* d_sync_ = nullptr;       // grid-barrier counter of the multi-level kernel
@@ -257,9 +279,13 @@ private:
     std::vector<cudaEvent_t> event_pool_;
     double timed_ms_ = 0;
     long long timed_launches_ = 0, timed_updates_ = 0;
+    // the same for the backward kernel (TimedRegion.launches < 0 marks them)
+    double btimed_ms_ = 0;
+    long long btimed_launches_ = 0, btimed_updates_ = 0;
 public:
     // plan used by the last forward propagation (for reporting)
     std::string last_fwd_plan;
+    std::string last_bwd_plan;
 };
 
 }  // namespace fwi

@@ -141,29 +141,14 @@ __device__ __forceinline__ void bwd_columns(const BwdArgs& a, const float* tsf, 
         const float4 ga = *reinterpret_cast<const float4*>(acc_a + off);
         const float4 gb = *reinterpret_cast<const float4*>(acc_b + off);
         const bool colok = !EDGE || (j >= 4 && j < nxx - 4);
-        float nps[4], npr[4], na[4], nb4[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const bool ok = !EDGE || (colok && ((rows.ok >> e) & 1u));
-            const float v = st::el(vv, e);
-            const float vp2 = v * v;
-            const float k = a.dt2idh2 * vp2;
-            const float s_new = k * ls[m][e] + 2.0f * st::el(psold[m], e) - st::el(ps, e);
-            const float r_new = k * lr[m][e] + 2.0f * st::el(pr[m], e) - st::el(prold, e);
-            nps[e] = ok ? s_new : 0.0f;
-            npr[e] = ok ? r_new : 0.0f;
-            const float prv = st::el(pr[m], e);
-            const float da = kGrad ? a.dt * prv * (ls[m][e] * a.idh2) * vp2 : s_new * prv;
-            const float db = s_new * s_new;
-            na[e] = st::el(ga, e) + (ok ? da : 0.0f);
-            nb4[e] = st::el(gb, e) + (ok ? db : 0.0f);
-        }
-        float4 rv = make_float4(npr[0], npr[1], npr[2], npr[3]);
+        const st::Bwd4 r = st::bwd_update4<kGrad, EDGE>(ls[m], psold[m], lr[m], pr[m], ps, prold, vv, ga, gb,
+                                                        a.dt2idh2, a.dt, a.idh2, rows, colok);
+        float4 rv = r.pr;
         if (has_rec) st::inject4(a.inj, a.inj.sample, sd.col_off, j, z, rv);
-        *reinterpret_cast<float4*>(a.ps_io + fo + off) = make_float4(nps[0], nps[1], nps[2], nps[3]);
+        *reinterpret_cast<float4*>(a.ps_io + fo + off) = r.ps;
         *reinterpret_cast<float4*>(a.pr_io + fo + off) = rv;
-        *reinterpret_cast<float4*>(acc_a + off) = make_float4(na[0], na[1], na[2], na[3]);
-        *reinterpret_cast<float4*>(acc_b + off) = make_float4(nb4[0], nb4[1], nb4[2], nb4[3]);
+        *reinterpret_cast<float4*>(acc_a + off) = r.a;
+        *reinterpret_cast<float4*>(acc_b + off) = r.b;
     }
 }
 

@@ -98,6 +98,30 @@ struct FwdTmaConfig {
     int S;    // pipeline stages
 };
 
+// Cooperative multi-level backward kernel (k_bwd_loop.cu): back-propagation
+// levels b_begin..b_end-1 of a batch in one launch.  Level b reads the source
+// field through the stencil from ps[(b+1)&1] and pointwise from ps[b&1] (and
+// overwrites it), the receiver field through the stencil from pr[b&1] and
+// pointwise from pr[(b+1)&1] (overwritten), as run_backward alternates them.
+struct BwdLoopArgs {
+    const ShotDesc* shots;
+    const int* tile_base;     // prefix sums of tiles per shot (ns+1)
+    int ns, ntz;
+    int ldz, nzz;
+    long long fstride;        // per-shot stride of fields, accumulators and velocity
+    int vel_shared;           // 1: one velocity for all shots
+    float dt2idh2, dt, idh2;
+    InjTable inj;             // receiver-side injection table of the batch
+    int nt;
+    int b_begin, b_end;
+    float* ps[2];
+    float* pr[2];
+    float* acc_a;
+    float* acc_b;
+    int* err;
+    unsigned* sync;           // grid-barrier counter, zero at launch
+};
+
 struct BwdArgs {
     const ShotDesc* shots;
     const float* vel;

@@ -40,6 +40,19 @@ cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S);
 cudaError_t launch_fwd_loop(int TX, int S, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
                             cudaStream_t st);
 
+// ---- k_bwd_loop.cu -------------------------------------------------------------
+// Tensor maps of the backward kernel: stencil boxes (128+8 rows, TX+8 columns)
+// and pointwise boxes (128 rows, TX columns), indexed like BwdLoopArgs.ps/pr.
+struct BwdLoopMaps {
+    CUtensorMap ps_st[2], pr_st[2];  // [p]: the buffer read through the stencil at parity p
+    CUtensorMap ps_pt[2], pr_pt[2];  // [p]: the buffer read and written pointwise at parity p
+    CUtensorMap acc_a, acc_b, vel;
+};
+bool bwd_loop_supported(int TX, int S);
+cudaError_t bwd_loop_configure(int* ctas_per_sm, int TX, int S);
+cudaError_t launch_bwd_loop(int TX, int S, bool gradient, const BwdLoopMaps& maps, const BwdLoopArgs& la, int grid,
+                            cudaStream_t st);
+
 // ---- k_rbc.cu ----------------------------------------------------------------
 struct BumpDev { float xc, zc, r, A, factor; };
 struct RbcArgs {
@@ -92,6 +105,17 @@ void launch_check_finite(const float* x, size_t n, int* flag, cudaStream_t st);
 // (the injection of time level 0, before the first step).
 void launch_inject_points(float* field, long long fstride, const ShotDesc* shots, int nshots, InjTable inj,
                           int ldz, cudaStream_t st);
+
+// ---- k_prep.cu -------------------------------------------------------------------
+// Direct-wave mute of nsrc seismograms (nrec x nt trace-major each) in place;
+// bits: nsrc scratch words.  Geometry arrays are on the device.
+void launch_mute_direct(float* data, int nsrc, int nrec, int nt, const float* sx, const float* sz, const float* rx,
+                        const float* rz, float velocity, float delay, float dt, float gstd, unsigned* bits,
+                        cudaStream_t st);
+// out = 1 / G(1 / vp) below row keep_rows, vp above; weights[0..radius] the
+// half of the normalised Gaussian; tmp: nz*nx scratch.
+void launch_smooth_slowness(const float* vp, int nz, int nx, const double* weights, int radius, int keep_rows,
+                            float* tmp, float* out, cudaStream_t st);
 
 // ---- k_noalloc.cu --------------------------------------------------------------
 size_t noalloc_max_samples();

@@ -122,6 +122,44 @@ __device__ __forceinline__ float4 update4(const float l[4], const float4& q, con
     return make_float4(out[0], out[1], out[2], out[3]);
 }
 
+// One float4 of the backward step (cross_correlation / build_gradient,
+// migration.cu:138-180, inversion.cu:405-444): the source field steps back,
+// the receiver field forward, and image (Ps_new * Pr) or gradient
+// (dt * Pr * lap(Psold) * v^2) and illumination (Ps_new^2) accumulate, only
+// inside 4 <= i < nzz-4, 4 <= j < nxx-4 (colok and rows.ok).
+struct Bwd4 {
+    float4 ps, pr, a, b;
+};
+template <bool GRAD, bool EDGE>
+__device__ __forceinline__ Bwd4 bwd_update4(const float ls[4], const float4& psold, const float lr[4],
+                                            const float4& pr, const float4& ps, const float4& prold,
+                                            const float4& vv, const float4& ga, const float4& gb, float dt2idh2,
+                                            float dt, float idh2, const Rows& rows, bool colok) {
+    float nps[4], npr[4], na[4], nb4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const bool ok = !EDGE || (colok && ((rows.ok >> e) & 1u));
+        const float v = el(vv, e);
+        const float vp2 = v * v;
+        const float k = dt2idh2 * vp2;
+        const float s_new = k * ls[e] + 2.0f * el(psold, e) - el(ps, e);
+        const float r_new = k * lr[e] + 2.0f * el(pr, e) - el(prold, e);
+        nps[e] = ok ? s_new : 0.0f;
+        npr[e] = ok ? r_new : 0.0f;
+        const float prv = el(pr, e);
+        const float da = GRAD ? dt * prv * (ls[e] * idh2) * vp2 : s_new * prv;
+        const float db = s_new * s_new;
+        na[e] = el(ga, e) + (ok ? da : 0.0f);
+        nb4[e] = el(gb, e) + (ok ? db : 0.0f);
+    }
+    Bwd4 r;
+    r.ps = make_float4(nps[0], nps[1], nps[2], nps[3]);
+    r.pr = make_float4(npr[0], npr[1], npr[2], npr[3]);
+    r.a = make_float4(na[0], na[1], na[2], na[3]);
+    r.b = make_float4(nb4[0], nb4[1], nb4[2], nb4[3]);
+    return r;
+}
+
 // Point injections of column j into rows z..z+3 (series sample `sample`).
 __device__ __forceinline__ void inject4(const InjTable& inj, int sample, int col_off, int j, int z, float4& v) {
     if (sample < 0) return;

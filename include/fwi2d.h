@@ -168,6 +168,23 @@ int  fwi_optimization(fwi_ctx* ctx, float f0, float* step);
  * m -= step*g; velocity = 1/sqrt(m).  vp_out (nz x nx) may be NULL. */
 int  fwi_update_model(fwi_ctx* ctx, float step, float* vp_out);
 
+/* ---- data preparation ----------------------------------------------------
+ * The reference prepares RTM input and the FWI starting model in Python;
+ * these run the same arithmetic on the GPU.
+ * fwi_mute_direct: run/generate_input_data.py:22-44 on all shots of data_all
+ * (nsrc x nt x nrec, in place): each shot divided by its max |amplitude|,
+ * samples t < tId[r] = int((dist_r / velocity + delay) / dt) of trace r
+ * tapered by exp(-0.5 ((t - tId[r]) / gstd)^2), dist_r the source-receiver
+ * distance from SPS/RPS.  The script's constants: velocity 3600, delay 0.18,
+ * gstd 30 (samples). */
+int  fwi_mute_direct(fwi_ctx* ctx, float* data_all, float velocity, float delay, float gstd);
+int  fwi_mute_direct_dev(fwi_ctx* ctx, float* d_data_all, float velocity, float delay, float gstd);
+/* run/generate_setup.py:49-51: vp_out = 1 / G(1 / vp) with G the separable
+ * Gaussian filter of scipy.ndimage (sigma in cells, radius int(4 sigma + 0.5),
+ * mode 'reflect', z pass then x pass), rows above int(depth_mask / dh) kept
+ * from vp.  nz x nx host arrays; the script uses sigma 3. */
+int  fwi_smooth_model(fwi_ctx* ctx, const float* vp, float sigma, float depth_mask, float* vp_out);
+
 /* ---- random boundary ----------------------------------------------------
  * set_random_boundary (modeling.cu:431-531) for shot `shot` of the current
  * model, on the context's RBC grid; out is nzz x (w + 2 nb) (z fastest,
@@ -218,7 +235,7 @@ int  fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, 
 int  fwi_describe(fwi_ctx* ctx, char* buf, size_t len);
 /* Kernel launches issued by the context since creation (or the last reset). */
 int  fwi_launch_count(fwi_ctx* ctx, long long* count, int reset);
-/* Forward-kernel timing.  fwi_fwd_timing(ctx, 1) resets the counters and
+/* Kernel timing.  fwi_fwd_timing(ctx, 1) resets the counters and
    brackets every later launch of the forward propagation kernel (a
    multi-level launch, or the graph of one-level launches of a batch) with
    CUDA events on the context stream; 0 turns it off.  fwi_fwd_timing_read
@@ -227,6 +244,9 @@ int  fwi_launch_count(fwi_ctx* ctx, long long* count, int reset);
    they performed (padded points x time levels x shots). */
 int  fwi_fwd_timing(fwi_ctx* ctx, int enable);
 int  fwi_fwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates);
+/* The same for the backward (migration / gradient) kernel, timed while
+ * fwi_fwd_timing is on. */
+int  fwi_bwd_timing_read(fwi_ctx* ctx, double* ms, long long* launches, long long* updates);
 
 #ifdef __cplusplus
 }

@@ -236,6 +236,39 @@ def rbc(base: np.ndarray, nb: int, dh: float, varVp: float, vmin: float, vmax: f
     return out.reshape(nxx, nzz).T
 
 
+# --------------------------------------------------------- data preparation
+def mute_direct(data: np.ndarray, sps: np.ndarray, rps: np.ndarray, dt: float, velocity=3600, time_delay=0.18,
+                gstd=30) -> np.ndarray:
+    """run/generate_input_data.py:22-44 on (nsrc, nt, nrec) seismograms with the
+    script's numpy dtypes: float32 data and geometry, Python scalars, the taper
+    in float64 (numpy's in-place multiply rounds the product to float32)."""
+    out = np.array(data, dtype=np.float32, copy=True)
+    sps = np.asarray(sps, np.float32)
+    rps = np.asarray(rps, np.float32)
+    nt = out.shape[1]
+    t = np.arange(nt)
+    for s in range(out.shape[0]):
+        d = out[s]
+        d *= 1.0 / np.max(np.abs(d))
+        dist = np.sqrt((rps[:, 0] - sps[s, 0]) ** 2 + (rps[:, 1] - sps[s, 1]) ** 2)
+        tid = np.array((dist / velocity + time_delay) / dt, dtype=int)
+        for r in range(out.shape[2]):
+            k = tid[r]
+            d[:k, r] *= np.exp(-0.5 * ((t - k) / gstd) ** 2)[:k]
+    return out
+
+
+def smooth_init(model: np.ndarray, sigma: float, depth_mask: float, dh: float) -> np.ndarray:
+    """run/generate_setup.py:49-51: 1 / gaussian_filter(1 / model, sigma), the
+    rows above int(depth_mask / dh) kept (scipy.ndimage, the script's own call)."""
+    from scipy.ndimage import gaussian_filter
+    m = np.asarray(model, np.float32)
+    out = 1.0 / gaussian_filter(1.0 / m, sigma)
+    z = int(depth_mask / dh)
+    out[:z] = m[:z]
+    return out.astype(np.float32)
+
+
 # --------------------------------------------------------- post-processing
 def image_post(img: np.ndarray, illum: np.ndarray, idh2: float) -> np.ndarray:
     q = (img.astype(np.float32) / illum.astype(np.float32)).astype(np.float32)

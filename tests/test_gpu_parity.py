@@ -144,10 +144,12 @@ def _rtm_data(c, vp):
     return np.stack(_oracle_modeling(c, vp, 20, 0.004, 64)).astype(np.float32)
 
 
-@pytest.mark.parametrize("variant", ["auto", "simple", "tma:2,16,2", "tma:1,32,2", "loop:16,2"])
-def test_rtm_vs_oracle(case, tmp_path, variant):
+@pytest.mark.parametrize("variant,bwd", [("auto", "auto"), ("simple", "simple"), ("tma:2,16,2", "loop:16,3"),
+                                         ("tma:1,32,2", "loop:16,2"), ("loop:16,2", "loop:8,4"),
+                                         ("loop:32,2", "loop:8,3")])
+def test_rtm_vs_oracle(case, tmp_path, variant, bwd):
     c0, vp = case
-    c, _ = synth.small_case(tmp_path, fwd_kernel=variant)
+    c, _ = synth.small_case(tmp_path, fwd_kernel=variant, bwd_kernel=bwd)
     smooth = synth.smooth_model(vp, c.dh, 40.0)
     data = _rtm_data(c, vp)
     with api.Context(c.params, api.MODE_MIGRATION) as ctx:
@@ -213,6 +215,20 @@ def test_misfit_and_gradient_vs_oracle(fwi_state):
     post = O.gradient_post(st["graw"], st["gill"], 1.0 / c.dh**2, int(float(c.keys["depth_mask"]) / c.dh))
     assert rel_l2(st["g"], post) < 1e-5
     assert abs(np.abs(st["g"]).max() - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("bwd", ["simple", "loop:16,3", "loop:16,2", "loop:8,4", "loop:8,3"])
+def test_gradient_backward_variants_agree(fwi_state, tmp_path, bwd):
+    """Every backward kernel gives the raw gradient of the fixture (auto plan)."""
+    st = fwi_state
+    c, _ = synth.small_case(tmp_path, bwd_kernel=bwd)
+    with api.Context(c.params, api.MODE_INVERSION) as ctx:
+        ctx.set_model(st["init"])
+        ctx.set_observed(st["obs"])
+        assert abs(ctx.compute_gradient(True) - st["sum_res"]) <= 1e-12 * st["sum_res"]
+        g, ill = ctx.gradient_raw()
+    assert rel_l2(g, st["graw"]) < 1e-5, bwd
+    assert rel_l2(ill, st["gill"]) < 1e-5, bwd
 
 
 def test_linesearch_optimization_update(fwi_state):
