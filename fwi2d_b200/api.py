@@ -56,6 +56,30 @@ SIGNATURES = {
     "fwi_get_wavelet": (C.c_int, [_P, _F]),
     "fwi_get_indices": (C.c_int, [_P, C.c_int, _I, _I, _I]),
     "fwi_get_window": (C.c_int, [_P, C.c_int, _I, _I]),
+    "fwi_set_direction": (C.c_int, [_P, _F]),
+    "fwi_update_model_bounded": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, _F]),
+    "fwi_set_direction_dev": (C.c_int, [_P, C.c_void_p]),
+    # fwi2d_nn.h (device pointers as integers)
+    "fwi_nn_conv3x3": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                 C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fwi_nn_wgrad_partial_floats": (C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "fwi_nn_conv3x3_wgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fwi_nn_weight_prep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fwi_nn_pool2": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "fwi_nn_pool2_bwd": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "fwi_nn_upcat": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                               C.c_void_p, C.c_void_p]),
+    "fwi_nn_upcat_bwd": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "fwi_nn_relu_bwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "fwi_nn_mse": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p,
+                             C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fwi_nn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.c_float,
+                              C.c_float, C.c_float, C.c_int, C.c_void_p]),
+    "fwi_nn_pack_inputs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fwi_nn_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p]),
     "fwi_mute_direct": (C.c_int, [_P, _F, C.c_float, C.c_float, C.c_float]),
     "fwi_mute_direct_dev": (C.c_int, [_P, C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "fwi_smooth_model": (C.c_int, [_P, _F, C.c_float, C.c_float, _F]),
@@ -316,10 +340,20 @@ class Context:
     def set_observed_raw(self, flat: np.ndarray) -> None:
         self._check(self._lib.fwi_set_observed(self._h, _fptr(flat)))
 
+    def set_observed_dev(self, dev_ptr: int) -> None:
+        self._check(self._lib.fwi_set_observed_dev(self._h, C.c_void_p(dev_ptr)))
+
     def compute_gradient(self, with_gradient: bool = True) -> float:
         s = C.c_double()
         self._check(self._lib.fwi_compute_gradient(self._h, int(with_gradient), C.byref(s)))
         return s.value
+
+    def set_direction(self, d: np.ndarray) -> None:
+        src = np.ascontiguousarray(np.asarray(d, dtype=np.float32).T).ravel()
+        self._check(self._lib.fwi_set_direction(self._h, _fptr(src)))
+
+    def set_direction_dev(self, dev_ptr: int) -> None:
+        self._check(self._lib.fwi_set_direction_dev(self._h, C.c_void_p(dev_ptr)))
 
     def gradient(self) -> np.ndarray:
         out = self._grid_out()
@@ -373,6 +407,11 @@ class Context:
     def update_model(self, step: float) -> np.ndarray:
         out = self._grid_out()
         self._check(self._lib.fwi_update_model(self._h, step, _fptr(out)))
+        return self._as2d(out)
+
+    def update_model_bounded(self, step: float, vmin: float, vmax: float) -> np.ndarray:
+        out = self._grid_out()
+        self._check(self._lib.fwi_update_model_bounded(self._h, step, vmin, vmax, _fptr(out)))
         return self._as2d(out)
 
     # -- data preparation (run/generate_input_data.py, run/generate_setup.py)

@@ -37,11 +37,12 @@ CU_SOURCES = {
     "k_fwd_loop.cu": [],
     "k_bwd_loop.cu": [],
     "k_prep.cu": ["-fmad=false"],
+    "k_nn.cu": [],
     "k_util.cu": [],
     "k_rbc.cu": ["-fmad=false"],
     "k_noalloc.cu": [],
 }
-CXX_SOURCES = ["host.cpp", "engine.cpp", "capi.cpp"]
+CXX_SOURCES = ["host.cpp", "engine.cpp", "capi.cpp", "capi_nn.cpp"]
 APPS = ["modeling", "migration", "inversion"]
 
 

@@ -232,6 +232,14 @@ int fwi_parabola_step(fwi_ctx* ctx, float f0, float f1, float f2, float* step) {
     return guarded(ctx, [&](fwi::Engine& e) { *step = e.parabola_step(f0, f1, f2); });
 }
 
+int fwi_set_direction(fwi_ctx* ctx, const float* dir) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.set_direction(dir, false); });
+}
+
+int fwi_set_direction_dev(fwi_ctx* ctx, const float* d_dir) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.set_direction(d_dir, true); });
+}
+
 int fwi_get_gradient(fwi_ctx* ctx, float* g) {
     if (!g) return arg_error(ctx, "NULL gradient");
     return guarded(ctx, [&](fwi::Engine& e) { e.get_gradient(g); });
@@ -267,6 +275,10 @@ int fwi_mute_direct_dev(fwi_ctx* ctx, float* d_data_all, float velocity, float d
 
 int fwi_smooth_model(fwi_ctx* ctx, const float* vp, float sigma, float depth_mask, float* vp_out) {
     return guarded(ctx, [&](fwi::Engine& e) { e.smooth_model(vp, sigma, depth_mask, vp_out); });
+}
+
+int fwi_update_model_bounded(fwi_ctx* ctx, float step, float vmin, float vmax, float* vp_out) {
+    return guarded(ctx, [&](fwi::Engine& e) { e.update_model(step, vp_out, vmin, vmax); });
 }
 
 int fwi_random_boundary(fwi_ctx* ctx, int shot, float* vp_rbc) {

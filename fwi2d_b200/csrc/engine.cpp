@@ -1492,6 +1492,20 @@ double Engine::compute_gradient(bool with_gradient) {
     return sum;
 }
 
+void Engine::set_direction(const float* dir, bool on_device) {
+    if (mode_ != FWI_MODE_INVERSION) throw Error(FWI_ERR_STATE, "a search direction needs an inversion context");
+    if (!dir) throw Error(FWI_ERR_ARG, "NULL direction");
+    const size_t n = (size_t)nx_ * nz_;
+    check(cudaMemcpyAsync(d_grad_, dir, n * sizeof(float),
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_),
+          "set direction");
+    launch_absmax(d_grad_, n, d_gmax_, st_);
+    launch_scale_by_inverse(d_grad_, n, d_gmax_, st_);
+    launches_ += 2;
+    have_grad_ = true;
+    sync("set_direction");
+}
+
 void Engine::get_gradient(float* g) {
     if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
     check(cudaMemcpyAsync(g, d_grad_, (size_t)nx_ * nz_ * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy gradient");
@@ -1556,10 +1570,13 @@ float Engine::optimization(float f0) {
     return 0.5f * (num / den);
 }
 
-void Engine::update_model(float step, float* vp_out) {
+void Engine::update_model(float step, float* vp_out, float vmin, float vmax) {
     if (!have_grad_) throw Error(FWI_ERR_STATE, "no gradient computed");
+    if (vmin != 0.0f && !(vmin > 0.0f && vmax > vmin)) throw Error(FWI_ERR_ARG, "bounds need 0 < vmin < vmax");
     const size_t npts = (size_t)nx_ * nz_;
-    launch_update_model(d_m_, d_grad_, step, d_vp_, npts, st_);
+    const float mlo = vmin > 0.0f ? 1.0f / (vmax * vmax) : 0.0f;
+    const float mhi = vmin > 0.0f ? 1.0f / (vmin * vmin) : 0.0f;
+    launch_update_model(d_m_, d_grad_, step, d_vp_, npts, st_, mlo, mhi);
     ++launches_;
     vel_abc_valid_ = vel_rbc_valid_ = false;
     if (vp_out) check(cudaMemcpyAsync(vp_out, d_vp_, npts * sizeof(float), cudaMemcpyDeviceToHost, st_), "copy model");

@@ -72,10 +72,14 @@ public:
     void trial_steps(float* a1, float* a2) const;
     float parabola_step(float f0, float f1, float f2) const;
     void get_gradient(float* g_host);
+    // replaces the search direction of the line search / update (normalised
+    // by its max |d| like the gradient): d_dir or host dir, nz x nx
+    void set_direction(const float* dir, bool on_device);
+    float* direction_dev() const { return d_grad_; }
     void get_gradient_raw(float* g_host, float* illum_host);
     double linesearch_trial(float alpha);
     float optimization(float f0);
-    void update_model(float step, float* vp_out);
+    void update_model(float step, float* vp_out, float vmin = 0.0f, float vmax = 0.0f);
     // data preparation (run/generate_input_data.py:22-44, run/generate_setup.py:49-51)
     void mute_direct(float* data_all, bool on_device, float velocity, float delay, float gstd);
     void smooth_model(const float* vp_host, float sigma, float depth_mask, float* out_host);

@@ -96,6 +96,14 @@ __global__ void grad_post_kernel(const float* __restrict__ g, const float* __res
     if ((threadIdx.x & 31) == 0) atomicMax(gmax_bits, __float_as_uint(local));
 }
 
+__global__ void absmax_kernel(const float* __restrict__ x, size_t n, unsigned int* bits) {
+    float m = 0.0f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(x[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(bits, __float_as_uint(m));
+}
+
 __global__ void scale_inv_kernel(float* x, size_t n, const unsigned int* gmax_bits) {
     const float inv = 1.0f / __uint_as_float(*gmax_bits);
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
@@ -143,9 +151,11 @@ __global__ void trial_kernel(const float* __restrict__ m, const float* __restric
     }
 }
 
-__global__ void update_kernel(float* m, const float* __restrict__ g, float step, float* __restrict__ vp, size_t n) {
+__global__ void update_kernel(float* m, const float* __restrict__ g, float step, float* __restrict__ vp, size_t n,
+                              float mlo, float mhi) {
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        const float nm = m[c] - step * g[c];
+        float nm = m[c] - step * g[c];
+        if (mlo > 0.0f) nm = fminf(fmaxf(nm, mlo), mhi);
         m[c] = nm;
         vp[c] = 1.0f / sqrtf(nm);
     }
@@ -213,6 +223,11 @@ void launch_grad_post(const float* g, const float* illum, int nz, int nx, float 
     grad_post_kernel<<<grid_for((size_t)nz * nx), 256, 0, st>>>(g, illum, nz, nx, idh2, zmask_i, out, gmax_bits);
 }
 
+void launch_absmax(const float* x, size_t n, unsigned int* bits, cudaStream_t st) {
+    cudaMemsetAsync(bits, 0, sizeof(unsigned int), st);
+    absmax_kernel<<<grid_for(n), 256, 0, st>>>(x, n, bits);
+}
+
 void launch_scale_by_inverse(float* x, size_t n, const unsigned int* gmax_bits, cudaStream_t st) {
     scale_inv_kernel<<<grid_for(n), 256, 0, st>>>(x, n, gmax_bits);
 }
@@ -230,8 +245,9 @@ void launch_trial_velocity(const float* m, const float* g, float alpha, float* v
     trial_kernel<<<grid_for(n), 256, 0, st>>>(m, g, alpha, vp, n);
 }
 
-void launch_update_model(float* m, const float* g, float step, float* vp, size_t n, cudaStream_t st) {
-    update_kernel<<<grid_for(n), 256, 0, st>>>(m, g, step, vp, n);
+void launch_update_model(float* m, const float* g, float step, float* vp, size_t n, cudaStream_t st, float mlo,
+                         float mhi) {
+    update_kernel<<<grid_for(n), 256, 0, st>>>(m, g, step, vp, n, mlo, mhi);
 }
 
 void launch_slowness2(const float* vp, float* m, size_t n, cudaStream_t st) {

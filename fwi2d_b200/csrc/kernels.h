@@ -88,6 +88,8 @@ void launch_rtm_post(const float* img, const float* illum, int nz, int nx, float
 void launch_grad_post(const float* g, const float* illum, int nz, int nx, float idh2, int zmask_i, float* out,
                       unsigned int* gmax_bits, cudaStream_t st);
 void launch_scale_by_inverse(float* x, size_t n, const unsigned int* gmax_bits, cudaStream_t st);
+// *bits = float bits of max |x| (order-independent, deterministic)
+void launch_absmax(const float* x, size_t n, unsigned int* bits, cudaStream_t st);
 // res = obs - cal over n samples, per-block FP64 partial sums of res^2 into
 // partial[], then a fixed-order sum into *out.  Deterministic.
 int  residual_blocks(size_t n);
@@ -96,7 +98,9 @@ void launch_residual(const float* obs, const float* cal, float* res, size_t n, d
 // vp = 1/sqrtf(m - alpha*g)  (inversion.cu:312-317)
 void launch_trial_velocity(const float* m, const float* g, float alpha, float* vp, size_t n, cudaStream_t st);
 // m -= step*g; vp = 1/sqrtf(m)  (inversion.cu:346-352)
-void launch_update_model(float* m, const float* g, float step, float* vp, size_t n, cudaStream_t st);
+// with mlo > 0 the new slowness^2 is clamped to [mlo, mhi]
+void launch_update_model(float* m, const float* g, float step, float* vp, size_t n, cudaStream_t st,
+                         float mlo = 0.0f, float mhi = 0.0f);
 // m = 1/(vp*vp)  (inversion.cu:101-109)
 void launch_slowness2(const float* vp, float* m, size_t n, cudaStream_t st);
 // Sets *flag to 1 when any of x[0..n) is not finite.
@@ -116,6 +120,28 @@ void launch_mute_direct(float* data, int nsrc, int nrec, int nt, const float* sx
 // half of the normalised Gaussian; tmp: nz*nx scratch.
 void launch_smooth_slowness(const float* vp, int nz, int nx, const double* weights, int radius, int keep_rows,
                             float* tmp, float* out, cudaStream_t st);
+
+// ---- k_nn.cu (CNN preconditioner; bf16 buffers passed as void*) ----------------
+int  nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
+                void* out, float* out32, cudaStream_t st);
+int  nn_wgrad_chunks(long long P);
+int  nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
+                      float* dw, float* db, cudaStream_t st);
+void nn_weight_prep(const float* w, int Cout, int Cin, void* wb, void* wt, cudaStream_t st);
+void nn_pool_fwd(const void* in, int N, int H, int W, int C, void* out, cudaStream_t st);
+void nn_pool_bwd(const float* dout, int N, int H, int W, int C, float* din, int accumulate, cudaStream_t st);
+void nn_upcat_fwd(const void* a, int Hs, int Ws, int C1, const void* skip, int N, int H, int W, int C2, void* out,
+                  cudaStream_t st);
+void nn_upcat_bwd(const float* dout, int N, int H, int W, int C1, int C2, int Hs, int Ws, float* da, int acc_a,
+                  float* dskip, int acc_skip, cudaStream_t st);
+void nn_relu_bwd(const float* da, const void* a, size_t n, void* dpre, cudaStream_t st);
+void nn_mse(const float* out32, int C, const float* target, const float* mask, long long P, float scale, void* dout,
+            double* partial, double* loss, cudaStream_t st);
+void nn_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps, int step,
+             cudaStream_t st);
+void nn_pack_inputs(const float* g, const float* il, const float* v, int nz, int nx, float v0, float vs,
+                    unsigned* bits, void* out, cudaStream_t st);
+void nn_unpack_channel(const float* out32, int C, long long P, float* dst, cudaStream_t st);
 
 // ---- k_noalloc.cu --------------------------------------------------------------
 size_t noalloc_max_samples();

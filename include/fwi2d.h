@@ -154,6 +154,12 @@ int  fwi_accumulators(fwi_ctx* ctx, float** d_image_or_gradient, float** d_illum
  * parabola vertex of misfits f0, f1, f2 at 0, a1, a2 (inversion.cu:286-308). */
 int  fwi_trial_steps(fwi_ctx* ctx, float* a1, float* a2);
 int  fwi_parabola_step(fwi_ctx* ctx, float f0, float f1, float f2, float* step);
+/* Replaces the search direction of fwi_linesearch_trial / fwi_optimization /
+ * fwi_update_model (m -= step * d) by dir (nz x nx, slowness^2 units),
+ * normalised by its max |d| as the gradient is: a preconditioned direction,
+ * e.g. the CNN's.  _dev: dir is a device pointer. */
+int  fwi_set_direction(fwi_ctx* ctx, const float* dir);
+int  fwi_set_direction_dev(fwi_ctx* ctx, const float* d_dir);
 /* Post-processed gradient (nz x nx, normalised by max |g|) */
 int  fwi_get_gradient(fwi_ctx* ctx, float* g);
 /* Raw gradient and illumination (nz x nx, cropped, before post-processing). */
@@ -167,6 +173,9 @@ int  fwi_optimization(fwi_ctx* ctx, float f0, float* step);
 /* Inversion::update_model (inversion.cu:344-358) without the file write:
  * m -= step*g; velocity = 1/sqrt(m).  vp_out (nz x nx) may be NULL. */
 int  fwi_update_model(fwi_ctx* ctx, float step, float* vp_out);
+/* The same with the new velocity kept inside [vmin, vmax] (no reference
+ * counterpart: the reference's update has no safeguard). */
+int  fwi_update_model_bounded(fwi_ctx* ctx, float step, float vmin, float vmax, float* vp_out);
 
 /* ---- data preparation ----------------------------------------------------
  * The reference prepares RTM input and the FWI starting model in Python;

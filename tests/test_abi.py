@@ -1,16 +1,19 @@
-"""The C-ABI library loads and exports every function include/fwi2d.h declares."""
+"""The C-ABI library loads and exports every function the headers in include/ declare."""
 import ctypes
 import re
 from pathlib import Path
 
 from fwi2d_b200 import api
 
-HEADER = Path(__file__).resolve().parent.parent / "include" / "fwi2d.h"
+HEADERS = sorted((Path(__file__).resolve().parent.parent / "include").glob("*.h"))
 
 
 def declared_functions() -> set[str]:
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    return set(re.findall(r"\b(fwi_\w+)\s*\(", text))
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(fwi_\w+)\s*\(", text))
+    return names
 
 
 def test_header_declares_the_boundary():
