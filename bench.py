@@ -205,6 +205,16 @@ def profile_case(which: str = "large"):
     fields ~630 MB > L2.  small: the benchmark survey once (L2-resident)."""
     from fwi2d_b200 import api, synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_prof_"))
+    if which == "batched":
+        # 60 of the 240 windowed shots (every 4th), nt 40: one RTM = one
+        # forward and one backward multi-level launch, fields ~1.9 GB > L2
+        case, _ = synth.config3(d, every=4, nt=40)
+        with api.Context(case.params, api.MODE_MIGRATION) as ctx:
+            dims = ctx.dims
+            ctx.rtm_reset()
+            ctx.rtm_survey_raw(np.zeros(dims.nsrc * dims.nrec * dims.nt, np.float32))
+            print("profile case done:", ctx.describe())
+        return
     if which == "small":
         case, _ = synth.config0(d, seed=0)
     else:
@@ -214,6 +224,41 @@ def profile_case(which: str = "large"):
         print("profile case done:", ctx.describe())
 
 
+def batched_survey(peak: float, nt: int = 300, reps: int = 2) -> dict:
+    """HBM-bound companion measurement: the batched uneven-aperture survey
+    (240 shots of the 301x1701 FWI model, each on its own window, all in one
+    batch), RTM through the random boundary with nt time samples; forward and
+    backward kernels timed by CUDA events on the engine stream."""
+    from fwi2d_b200 import api, synth
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_batched_"))
+    case, _ = synth.config3(d, nt=nt)
+    with api.Context(case.params, api.MODE_MIGRATION) as ctx:
+        dims = ctx.dims
+        widths = [ctx.window(s)[1] for s in range(dims.nsrc)]
+        data = np.zeros(dims.nsrc * dims.nrec * dims.nt, np.float32)
+        ctx.rtm_reset()
+        ctx.rtm_survey_raw(data)  # autotune + warm-up
+        ctx.fwd_timing(True)
+        for _ in range(reps):
+            ctx.rtm_survey_raw(data)
+        fms, fn, fu = ctx.fwd_timing_read()
+        bms, bn, bu = ctx.bwd_timing_read()
+        ctx.fwd_timing(False)
+        plan = ctx.describe()
+    fwd_gbs = 16 * fu / (fms * 1e-3) / 1e9
+    bwd_gbs = 44 * bu / (bms * 1e-3) / 1e9
+    return {
+        "workload": f"{dims.nsrc} shots of the 301x1701 FWI model, aperture windows {min(widths)}-{max(widths)} "
+                    f"columns (mean {np.mean(widths):.0f}) + 2x{dims.rbc_nb} boundary, {dims.nzz} rows, "
+                    f"{dims.nt + dims.tlag} levels, RTM through the random boundary",
+        "forward": {"updates_per_s": fu / (fms * 1e-3), "algorithmic_gbs": fwd_gbs, "frac": fwd_gbs / peak,
+                    "bytes_per_update": 16, "launches": fn, "ms": fms},
+        "backward": {"updates_per_s": bu / (bms * 1e-3), "algorithmic_gbs": bwd_gbs, "frac": bwd_gbs / peak,
+                     "bytes_per_update": 44, "launches": bn, "ms": bms},
+        "plans": plan,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -221,7 +266,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small"],
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-survey companion measurement")
+    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small", "batched"],
                     help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
                          "time axis; small: the benchmark survey)")
     args = ap.parse_args()
@@ -343,6 +389,9 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case, vp)
+    if world == 1 and not args.no_batched:
+        ctx.close()
+        line["batched_survey"] = batched_survey(peak)
     ctx.close()
     if world > 1:
         torch.distributed.barrier()

@@ -91,7 +91,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         exe = BIN / app
         src = CSRC / "apps" / f"{app}_main.cpp"
         if _stale(exe, [src, LIB, CSRC / "apps" / "app_common.hpp"]):
-            _run(["g++", "-O2", "-std=c++17", "-o", str(exe), str(src), f"-L{PKG}", "-lfwi2d",
+            _run(["g++", "-O2", "-std=c++17", "-pthread", "-o", str(exe), str(src), f"-L{PKG}", "-lfwi2d",
                   "-Wl,-rpath,$ORIGIN/.."])
     return LIB
 

@@ -1,9 +1,12 @@
 // app_common.hpp — helpers shared by the three drop-in executables.
 #pragma once
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/fwi2d.h"
@@ -37,15 +40,35 @@ inline bool read_floats(const std::string& path, float* dst, size_t n) {
     return true;
 }
 
-inline bool write_floats(const std::string& path, const float* src, size_t n) {
+inline bool write_floats(const std::string& path, const float* src, size_t n, bool announce = true) {
     std::ofstream f(path, std::ios::binary);
     if (!f.is_open()) {
         std::fprintf(stderr, "Error: %s could not be opened!\n", path.c_str());
         return false;
     }
     f.write(reinterpret_cast<const char*>(src), (std::streamsize)(n * sizeof(float)));
-    std::printf("\nBinary file %s was successfully written.\n", path.c_str());
+    if (announce) std::printf("\nBinary file %s was successfully written.\n", path.c_str());
     return (bool)f;
+}
+
+// Per-shot file I/O on a small pool of host threads (the reference reads and
+// writes one shot at a time, inversion.cu:168-172, modeling.cu:279-284): runs
+// fn(i) for i in [0, n) and returns whether every call succeeded.
+template <class F>
+bool parallel_files(int n, F fn) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int workers = std::max(1, std::min(n, (int)std::min(16u, hw)));
+    std::atomic<int> next{0};
+    std::atomic<bool> ok{true};
+    std::vector<std::thread> pool;
+    pool.reserve(workers);
+    for (int t = 0; t < workers; ++t)
+        pool.emplace_back([&] {
+            for (int i = next++; i < n; i = next++)
+                if (!fn(i)) ok = false;
+        });
+    for (auto& th : pool) th.join();
+    return ok;
 }
 
 inline std::string banner(const char* title) {

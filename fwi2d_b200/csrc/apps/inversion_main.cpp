@@ -30,12 +30,12 @@ int main(int argc, char** argv) {
 
     const size_t per = (size_t)d.nt * d.nrec;
     std::vector<float> obs(per * d.nsrc);
-    for (int s = 0; s < d.nsrc; ++s) {  // set_obs_data, inversion.cu:168-172
-        std::string file = in_folder + in_prefix + std::to_string(s + 1) + ".bin";
-        if (!app::read_floats(file, obs.data() + per * s, per)) {
-            fwi_ctx_destroy(ctx);
-            return 1;
-        }
+    // set_obs_data, inversion.cu:168-172: every shot's file, read in parallel
+    if (!app::parallel_files(d.nsrc, [&](int s) {
+            return app::read_floats(in_folder + in_prefix + std::to_string(s + 1) + ".bin", obs.data() + per * s, per);
+        })) {
+        fwi_ctx_destroy(ctx);
+        return 1;
     }
     if (fwi_set_observed(ctx, obs.data()) != FWI_OK) return app::fail(ctx, "set_obs_data");
 

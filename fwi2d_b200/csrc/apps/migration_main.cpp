@@ -26,12 +26,11 @@ int main(int argc, char** argv) {
     const size_t per = (size_t)d.nt * d.nrec;
     std::vector<float> data(per * d.nsrc);
     // set_seismic_source, migration.cu:83-88
-    for (int s = 0; s < d.nsrc; ++s) {
-        std::string file = in_folder + in_prefix + std::to_string(s + 1) + ".bin";
-        if (!app::read_floats(file, data.data() + per * s, per)) {
-            fwi_ctx_destroy(ctx);
-            return 1;
-        }
+    if (!app::parallel_files(d.nsrc, [&](int s) {
+            return app::read_floats(in_folder + in_prefix + std::to_string(s + 1) + ".bin", data.data() + per * s, per);
+        })) {
+        fwi_ctx_destroy(ctx);
+        return 1;
     }
     auto ti = app::clock::now();
     if (fwi_rtm_survey(ctx, data.data()) != FWI_OK) return app::fail(ctx, "migration");

@@ -27,13 +27,17 @@ int main(int argc, char** argv) {
     std::vector<float> seis(per * d.nsrc);
     auto ti = app::clock::now();
     if (fwi_model_survey(ctx, seis.data()) != FWI_OK) return app::fail(ctx, "forward_solver");
-    for (int s = 0; s < d.nsrc; ++s) {
-        char name[64];
-        std::snprintf(name, sizeof name, "%d", int(1e6f * d.dt));
-        std::string file = folder + "seismogram_nt" + std::to_string(d.nt) + "_nr" + std::to_string(d.nrec) + "_" +
-                           name + "us_shot_" + std::to_string(s + 1) + ".bin";
-        if (!app::write_floats(file, seis.data() + per * s, per)) return app::fail(ctx, "get_seismogram");
-    }
+    char us[64];
+    std::snprintf(us, sizeof us, "%d", int(1e6f * d.dt));
+    auto file_of = [&](int s) {
+        return folder + "seismogram_nt" + std::to_string(d.nt) + "_nr" + std::to_string(d.nrec) + "_" + us +
+               "us_shot_" + std::to_string(s + 1) + ".bin";
+    };
+    // get_seismogram for every shot, the files written by a thread pool
+    if (!app::parallel_files(d.nsrc,
+                             [&](int s) { return app::write_floats(file_of(s), seis.data() + per * s, per, false); }))
+        return app::fail(ctx, "get_seismogram");
+    for (int s = 0; s < d.nsrc; ++s) std::printf("\nBinary file %s was successfully written.\n", file_of(s).c_str());
     auto tf = app::clock::now();
     std::printf("\nRun time: %g s.\n", app::seconds(ti, tf));
     fwi_ctx_destroy(ctx);

@@ -87,13 +87,14 @@ VMIN, VMAX = 1400.0, 4800.0  # bounds of the safeguarded update (the model famil
 
 def line_search(ctx: api.Context, f0: float) -> tuple[float, float, float]:
     """Trials at a1, a2 along the context's direction; returns (step, f1, f2).
-    The step is the parabola's vertex when it is positive and at most 4 a2,
-    else the better trial when it cut the misfit, else 0."""
+    The step is the parabola's vertex (inversion.cu:286-308) when it is
+    positive and finite, else the better trial when it cut the misfit, else 0;
+    the bounded update keeps any step's model physical."""
     a1, a2 = ctx.trial_steps()
     f1 = float(np.sqrt(np.float32(ctx.linesearch_trial(a1))))
     f2 = float(np.sqrt(np.float32(ctx.linesearch_trial(a2))))
     step = ctx.parabola_step(f0, f1, f2)
-    if not (np.isfinite(step) and 0.0 < step <= 4.0 * a2):
+    if not (np.isfinite(step) and step > 0.0):
         fb, ab = min((f1, a1), (f2, a2))
         step = ab if fb < f0 else 0.0
     return step, f1, f2
@@ -245,3 +246,76 @@ def time_to_error(log: FwiLog, target: float) -> float | None:
         if e <= target:
             return t
     return None
+
+
+def main(argv=None) -> int:
+    """Train the preconditioner and compare CNN-preconditioned with plain FWI.
+
+    python -m fwi2d_b200.precond --models 128 --stages 4 --epochs 40 --iterations 10 --test small|config3
+    writes a JSON summary (--out) with the training history and both runs'
+    misfit, model-error and wall-time trajectories."""
+    import argparse
+    import json
+    import tempfile
+
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--models", type=int, default=128)
+    ap.add_argument("--stages", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--iterations", type=int, default=10)
+    ap.add_argument("--test", choices=["small", "config3"], default="small")
+    ap.add_argument("--nt", type=int, default=None, help="time samples of the config3 test (default 4001)")
+    ap.add_argument("--target", type=float, default=0.03)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--weights", default=None, help="save / load the trained network here")
+    a = ap.parse_args(argv)
+    root = Path(tempfile.mkdtemp(prefix="fwi2d_precond_"))
+    s = PairSetup()
+    res = {"setup": vars(a)}
+    net = cnn.UNet(seed=0)
+    t0 = time.perf_counter()
+    if a.weights and Path(a.weights).exists():
+        net.load(a.weights)
+        res["training"] = {"loaded": a.weights}
+    else:
+        X, T = make_pairs(root / "pairs", a.models, a.stages, setup=s)
+        t1 = time.perf_counter()
+        hist = train(net, X, T, s, epochs=a.epochs, batch=4, lr=1e-3, val=8 * a.stages)
+        t2 = time.perf_counter()
+        res["training"] = {"pairs": int(X.shape[0]), "pair_seconds": t1 - t0, "train_seconds": t2 - t1, **hist}
+        del X, T
+        if a.weights:
+            net.save(a.weights)
+    if a.test == "small":
+        vt = true_model(s, 7)
+        case = write_setup(root / "test", s, vt)
+        vs = start_model(vt, s.dh)
+    else:
+        kw = {"nt": a.nt} if a.nt else {}
+        case, vt = synth.config3(root / "test", **kw)
+        vs = synth.gradient_model(vt, case.dh)
+    runs = {}
+    for mode in ("plain", "cnn"):
+        with api.Context(case.params, api.MODE_INVERSION) as ctx:
+            d = ctx.dims
+            seis = torch.empty(d.nsrc * d.nrec * d.nt, dtype=torch.float32, device="cuda")
+            ctx.set_model(vt)
+            ctx.model_survey_dev(seis.data_ptr())
+            ctx.set_model(vs)
+            ctx.set_observed_dev(seis.data_ptr())
+            ctx.set_seed(7)
+            lg = fwi(ctx, vt, a.iterations, net if mode == "cnn" else None)
+            runs[mode] = {"residuo": lg.residuo, "model_error": lg.model_error, "seconds": lg.seconds,
+                          "direction": lg.direction, "time_to_target": time_to_error(lg, a.target)}
+    res["runs"] = runs
+    txt = json.dumps(res)
+    if a.out:
+        Path(a.out).write_text(txt)
+    print(txt)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -177,16 +177,18 @@ def config2(root, seed: int = 2, **over) -> tuple[Case, np.ndarray]:
     return case, vp
 
 
-def config3(root, seed: int = 3, **over) -> tuple[Case, np.ndarray]:
+def config3(root, seed: int = 3, every: int = 1, **over) -> tuple[Case, np.ndarray]:
     """Batched uneven-aperture FWI: the config-2 model and receiver spread,
     240 shots every 70 m, each modeled on the columns within its own maximum
-    offset (uniform 1.5-8 km from the seed; windows of about 300-1700 columns)."""
+    offset (uniform 1.5-8 km from the seed; windows of about 300-1700 columns).
+    every > 1 keeps every every-th shot (smaller profiling cases)."""
     nz, nx, dh = 301, 1701, 10.0
     vp = dipping_model(nz, nx, dh, 2)
     sx = np.arange(240) * 70.0 + 100.0
     rx = np.arange(851) * 20.0
     rng = np.random.default_rng(seed)
     offsets = rng.uniform(1500.0, 8000.0, sx.size).astype(np.float32)
+    sx, offsets = sx[::every], offsets[::every]
     kw = dict(nt=4001, dt=1e-3, fmax=15.0)
     kw.update({k: over.pop(k) for k in list(over) if k in kw})
     root = Path(root)
