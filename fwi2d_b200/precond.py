@@ -85,16 +85,23 @@ def features(ctx: api.Context, vp_dev, out) -> None:
 VMIN, VMAX = 1400.0, 4800.0  # bounds of the safeguarded update (the model family spans 1500-4800 m/s)
 
 
-def line_search(ctx: api.Context, f0: float) -> tuple[float, float, float]:
+STEP_CAP = 4.0  # largest step, in units of the second trial step a2
+
+
+def line_search(ctx: api.Context, f0: float, cap: float | None = STEP_CAP) -> tuple[float, float, float]:
     """Trials at a1, a2 along the context's direction; returns (step, f1, f2).
     The step is the parabola's vertex (inversion.cu:286-308) when it is
-    positive and finite, else the better trial when it cut the misfit, else 0;
-    the bounded update keeps any step's model physical."""
+    positive and finite, clipped to cap * a2 (the vertex of a parabola fitted
+    on [0, a2] extrapolates badly far beyond it; None: no clip), else the
+    better trial when it cut the misfit, else 0."""
     a1, a2 = ctx.trial_steps()
     f1 = float(np.sqrt(np.float32(ctx.linesearch_trial(a1))))
     f2 = float(np.sqrt(np.float32(ctx.linesearch_trial(a2))))
     step = ctx.parabola_step(f0, f1, f2)
-    if not (np.isfinite(step) and step > 0.0):
+    if np.isfinite(step) and step > 0.0:
+        if cap is not None:
+            step = min(step, cap * a2)
+    else:
         fb, ab = min((f1, a1), (f2, a2))
         step = ab if fb < f0 else 0.0
     return step, f1, f2
@@ -200,7 +207,8 @@ def model_error(v: np.ndarray, v_true: np.ndarray) -> float:
     return float(np.sqrt(np.mean((v - t) ** 2)) / np.sqrt(np.mean(t ** 2)))
 
 
-def fwi(ctx: api.Context, v_true: np.ndarray, iterations: int, net: cnn.UNet | None = None, log=print) -> FwiLog:
+def fwi(ctx: api.Context, v_true: np.ndarray, iterations: int, net: cnn.UNet | None = None, log=print,
+        cap: float | None = STEP_CAP) -> FwiLog:
     """Plain (net None) or CNN-preconditioned FWI from the context's model;
     both take the safeguarded step of line_search and the bounded update."""
     torch = _torch()
@@ -225,11 +233,11 @@ def fwi(ctx: api.Context, v_true: np.ndarray, iterations: int, net: cnn.UNet | N
             torch.cuda.synchronize()
             ctx.set_direction_dev(direction.data_ptr())
             used = "cnn"
-        step, f1, f2 = line_search(ctx, f0)
+        step, f1, f2 = line_search(ctx, f0, cap)
         if net is not None and (step <= 0.0 or min(f1, f2) >= f0):
             ctx.gradient_finish()  # back to the illumination-normalised gradient
             used = "fallback"
-            step, f1, f2 = line_search(ctx, f0)
+            step, f1, f2 = line_search(ctx, f0, cap)
         v = ctx.update_model_bounded(step, VMIN, VMAX)
         out.direction.append(used)
         out.model_error.append(model_error(v, v_true))
