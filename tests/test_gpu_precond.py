@@ -14,7 +14,7 @@ from fwi2d_b200 import api, cnn, precond
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-SETUP = precond.PairSetup(nz=64, nx=192, nt=1001, nshots=5, nrec=96, boundary=190.0)
+SETUP = precond.PairSetup(nz=96, nx=192, nt=1001, nshots=5, nrec=96, boundary=190.0)
 
 
 @pytest.fixture(scope="module")
