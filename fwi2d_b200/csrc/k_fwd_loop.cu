@@ -11,16 +11,10 @@
 // kernel, and the tensor maps of all four are kernel parameters.
 //
 // Grid barrier: after a CTA has written its tiles of a level, its first thread
-// fences, increments a global counter and polls it (bounded; a short sleep
-// after the first polls) until every CTA has arrived; the producer then issues
-// a proxy fence so its next TMA reads see the other CTAs' stores.  A poll that
-// gives up raises *err and the kernel returns with no copy in flight.
-//
-// The barrier only guards the Q^t tile with its halo, which neighbours write.
-// The pointwise inputs of a CTA's first S tiles of the next level (its own
-// Q^t tile, written a level earlier, and the velocity) do not depend on it, so
-// the producer issues those loads while the barrier is pending (expect_tx
-// without the arrival) and adds the halo'd load with the arrival after it.
+// fences, increments a global counter and polls it (bounded, with a short
+// sleep) until every CTA has arrived; the producer then issues a proxy fence so
+// its next TMA reads see the other CTAs' stores.  A poll that gives up raises
+// *err and the kernel returns with no copy in flight.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -43,27 +37,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target)
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
         if (v >= target) return true;
-        if (i >= 32) __nanosleep(64);
+        __nanosleep(64);
     }
     return false;
-}
-
-// Fills the metadata of one tile of a level: sample1 / rec_sample0 are the
-// level's source sample and recorded sample (-1 for none).
-__device__ __forceinline__ void fill_meta(TileMeta& mt, const FwdTmaArgs& a, const TileInfo& ti, const ShotDesc& sd,
-                                          int tx, int sample1, int rec_sample0) {
-    mt.s = ti.s;
-    mt.x0 = ti.x0;
-    mt.z0 = ti.z0;
-    mt.nxx = sd.nxx;
-    mt.col_off = sd.col_off;
-    mt.has_src = sample1 >= 0 && st::has_points(a.inj, sd.col_off, ti.x0, min(ti.x0 + tx, sd.nxx));
-    if (rec_sample0 >= 0 && a.seis) {
-        mt.rec_kb = __ldg(a.rec.colptr + sd.col_off + ti.x0);
-        mt.rec_ke = __ldg(a.rec.colptr + sd.col_off + min(ti.x0 + tx, sd.nxx));
-    } else {
-        mt.rec_kb = mt.rec_ke = 0;
-    }
 }
 
 __device__ __forceinline__ void fence_proxy_async_global() {
@@ -95,10 +71,7 @@ __global__ void __launch_bounds__(kNT, 2)
     __syncthreads();
 
     const int lane = tid & 31;
-    // tiles of this CTA per level (the same at every level)
-    const int ntile = total > (int)blockIdx.x ? (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     int issued = 0;  // producer lane: loads issued so far (pipeline uses)
-    int pre = 0;     // producer lane: first tiles of the level whose pointwise loads are in flight
     int k = 0;       // pipeline use counter, continuous across levels
     int c = la.buf_cur, o = la.buf_old, f = la.buf_free;
     for (int t = la.t_begin; t < la.t_end; ++t) {
@@ -115,23 +88,29 @@ __global__ void __launch_bounds__(kNT, 2)
             if (lane == 0) {
                 fence_proxy_async_global();
                 int kk = k;
-                for (int tile = blockIdx.x, i = 0; tile < total; tile += gridDim.x, ++kk, ++i) {
+                for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                     const int stg = kk % S;
-                    float* base = smem + stg * G::STAGE;
-                    if (i < pre) {
-                        // metadata and pointwise loads issued while the barrier was pending
-                        const TileMeta& mt = meta[stg];
-                        tma::mbar_arrive_expect_tx(&full[stg], G::CUR * 4);
-                        tma::load_3d(base, &maps.cur[c], mt.z0 - 4, mt.x0 - 4, mt.s, &full[stg]);
-                        continue;
-                    }
                     if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1))) {
                         ok = false;
                         break;
                     }
                     const TileInfo ti = decode(a, tile, TX);
                     const ShotDesc sd = a.shots[ti.s];
-                    fill_meta(meta[stg], a, ti, sd, TX, a.sample1, a.rec_sample0);
+                    TileMeta& mt = meta[stg];
+                    mt.s = ti.s;
+                    mt.x0 = ti.x0;
+                    mt.z0 = ti.z0;
+                    mt.nxx = sd.nxx;
+                    mt.col_off = sd.col_off;
+                    mt.has_src = a.sample1 >= 0 &&
+                                 st::has_points(a.inj, sd.col_off, ti.x0, min(ti.x0 + TX, sd.nxx));
+                    if (a.rec_sample0 >= 0 && a.seis) {
+                        mt.rec_kb = __ldg(a.rec.colptr + sd.col_off + ti.x0);
+                        mt.rec_ke = __ldg(a.rec.colptr + sd.col_off + min(ti.x0 + TX, sd.nxx));
+                    } else {
+                        mt.rec_kb = mt.rec_ke = 0;
+                    }
+                    float* base = smem + stg * G::STAGE;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
                     tma::load_3d(base, &maps.cur[c], ti.z0 - 4, ti.x0 - 4, ti.s, &full[stg]);
                     tma::load_3d(base + G::CUR, &maps.pt[o], ti.z0, ti.x0, ti.s, &full[stg]);
@@ -139,7 +118,6 @@ __global__ void __launch_bounds__(kNT, 2)
                                  a.vel_shared ? 0 : ti.s, &full[stg]);
                     issued = kk + 1;
                 }
-                pre = 0;
                 if (!ok) {
                     atomicExch(a.err, 1);
                     abort_flag = 1;
@@ -198,26 +176,6 @@ __global__ void __launch_bounds__(kNT, 2)
         }
         // the CTA's tiles of level t are written: grid barrier
         __syncthreads();
-        if (tid == kNC && !abort_flag && t + 1 < la.t_end) {
-            // every stage is free: issue the pointwise loads of the next
-            // level's first tiles (Q^t of this CTA's own tiles is buffer c,
-            // written a level ago) while the barrier completes
-            const int s1 = (t + 2 < la.nt) ? t + 2 : -1;
-            const int r0 = (la.record && t + 1 > la.tlag) ? t + 1 - la.tlag : -1;
-            int kk = k + ntile;
-            for (int tile = blockIdx.x; tile < total && pre < S; tile += gridDim.x, ++kk, ++pre) {
-                const int stg = kk % S;
-                float* base = smem + stg * G::STAGE;
-                const TileInfo ti = decode(a, tile, TX);
-                const ShotDesc sd = a.shots[ti.s];
-                fill_meta(meta[stg], a, ti, sd, TX, s1, r0);
-                tma::mbar_expect_tx(&full[stg], 2 * G::PTW * 4);
-                tma::load_3d(base + G::CUR, &maps.pt[c], ti.z0, ti.x0, ti.s, &full[stg]);
-                tma::load_3d(base + G::CUR + G::PTW, &maps.vel, ti.z0, ti.x0 + sd.vel_col, a.vel_shared ? 0 : ti.s,
-                             &full[stg]);
-            }
-            issued = kk;
-        }
         if (tid == 0 && !abort_flag) {
             if (!grid_barrier(la.sync, (unsigned)(t - la.t_begin + 1) * gridDim.x)) {
                 atomicExch(b.err, 1);
@@ -226,14 +184,11 @@ __global__ void __launch_bounds__(kNT, 2)
         }
         __syncthreads();
         if (abort_flag) {
-            // never leave copies in flight behind an exiting CTA: complete the
-            // phases of the prefetched stages (their arrival is still due),
-            // then wait (bounded) for the last S loads issued
-            if (tid == kNC) {
-                for (int q = issued - pre; q < issued; ++q) tma::mbar_arrive(&full[q % S]);
+            // never leave copies in flight behind an exiting CTA: wait (bounded)
+            // for the last S loads issued; phases already consumed pass at once
+            if (tid == kNC)
                 for (int q = (issued > S ? issued - S : 0); q < issued; ++q)
                     tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
-            }
             return;
         }
         // this CTA's tile count per level is fixed: advance the pipeline counter
