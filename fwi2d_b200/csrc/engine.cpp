@@ -760,7 +760,7 @@ void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Table
     check(cudaMemsetAsync(d_sync_, 0, sizeof(unsigned), st_), "memset grid barrier");
     TimedRegion r;
     if (timed_updates >= 0) timing_begin(&r);
-    check(launch_fwd_loop(TX, p.cfg.S, maps, la, p.grid, st_), "multi-level forward launch");
+    check(launch_fwd_loop(TX, p.cfg.S, p.minb, maps, la, p.grid, st_), "multi-level forward launch");
     if (timed_updates >= 0) timing_end(&r, 1, timed_updates);
     ++launches_;
 }
@@ -791,12 +791,13 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         p.tail_grid = sm_count_ * ctas_t;
         return p;
     };
-    auto make_loop = [&](int TX, int S) {
+    auto make_loop = [&](int TX, int S, int B) {
         FwdPlan p;
         p.kind = 2;
         p.cfg = FwdTmaConfig{1, TX, S};
+        p.minb = B;
         int ctas = 0;
-        if (fwd_loop_configure(&ctas, TX, S) != cudaSuccess || ctas < 1) {
+        if (fwd_loop_configure(&ctas, TX, S, B) != cudaSuccess || ctas < 1) {
             cudaGetLastError();
             p.kind = -1;
             return p;
@@ -813,18 +814,19 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
             throw Error(FWI_ERR_PARAM, "fwd_kernel '" + fwd_kernel_ + "' is not a compiled TMA variant");
         cands.push_back(make(T, TX, S));
     } else if (fwd_kernel_.rfind("loop:", 0) == 0) {
-        int TX = 0, S = 0;
-        if (std::sscanf(fwd_kernel_.c_str() + 5, "%d,%d", &TX, &S) != 2 || !fwd_loop_supported(TX, S))
+        int TX = 0, S = 0, B = 2;
+        const int got = std::sscanf(fwd_kernel_.c_str() + 5, "%d,%d,%d", &TX, &S, &B);
+        if (got < 2 || !fwd_loop_supported(TX, S, B))
             throw Error(FWI_ERR_PARAM, "fwd_kernel '" + fwd_kernel_ + "' is not a compiled multi-level variant");
-        cands.push_back(make_loop(TX, S));
+        cands.push_back(make_loop(TX, S, B));
     } else if (fwd_kernel_ == "auto" || fwd_kernel_ == "tma") {
         if (fwd_kernel_ == "auto") cands.push_back(FwdPlan{});
         const int variants[][3] = {{1, 32, 2}, {1, 32, 3}, {1, 16, 3}, {1, 16, 4}, {2, 32, 2}, {2, 16, 2}, {2, 16, 3}};
         for (const auto& v : variants) cands.push_back(make(v[0], v[1], v[2]));
-        const int loops[][2] = {{32, 2}, {16, 3}, {16, 2}};
-        for (const auto& v : loops) cands.push_back(make_loop(v[0], v[1]));
+        const int loops[][3] = {{32, 2, 2}, {16, 3, 2}, {16, 2, 2}, {16, 2, 3}};
+        for (const auto& v : loops) cands.push_back(make_loop(v[0], v[1], v[2]));
     } else {
-        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma, tma:T,TX,S or loop:TX,S");
+        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma, tma:T,TX,S or loop:TX,S[,B]");
     }
     FwdPlan best;
     double best_us = 1e30;
@@ -837,7 +839,7 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         }
         c.us_per_step = time_fwd_candidate(c, g, t, ns, vel, vel_stride, abc);
         if (c.kind == 0) log << " simple=" << c.us_per_step;
-        else if (c.kind == 2) log << " loop" << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
+        else if (c.kind == 2) log << " loop" << c.cfg.TX << "," << c.cfg.S << "," << c.minb << "=" << c.us_per_step;
         else log << " tma" << c.cfg.T << "," << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
         if (c.us_per_step < best_us) {
             best_us = c.us_per_step;
@@ -857,7 +859,8 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     {
         std::ostringstream d;
         if (plan.kind == 0) d << "simple";
-        else if (plan.kind == 2) d << "loop TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
+        else if (plan.kind == 2)
+            d << "loop TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " B=" << plan.minb << " grid=" << plan.grid;
         else d << "tma T=" << plan.cfg.T << " TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
         if (!plan.tuning.empty()) d << " | us/step:" << plan.tuning;
         last_fwd_plan = d.str();

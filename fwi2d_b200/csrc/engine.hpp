@@ -139,10 +139,11 @@ private:
     // forward-kernel choice for (grid, batch size, ABC): the simple tiled kernel
     // (k_stencil.cu) or a persistent TMA variant (k_fwd_tma.cu), autotuned
     struct FwdPlan {
-        int kind = 0;                 // 0 simple, 1 TMA
+        int kind = 0;                 // 0 simple, 1 TMA (per-launch), 2 multi-level
         FwdTmaConfig cfg{1, 32, 2};
         FwdTmaConfig tail{1, 32, 2};  // T = 1 variant for an odd last step
         int grid = 0, tail_grid = 0;
+        int minb = 2;                 // multi-level kernel: CTAs per SM of its register budget
         double us_per_step = 0;
         std::string tuning;           // autotuner timings of all candidates
     };

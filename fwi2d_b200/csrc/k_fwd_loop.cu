@@ -46,8 +46,9 @@ __device__ __forceinline__ void fence_proxy_async_global() {
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
-template <int TX, int S, bool ABC>
-__global__ void __launch_bounds__(kNT, 2)
+// MINB: CTAs per SM the registers are budgeted for (shared memory permitting)
+template <int TX, int S, bool ABC, int MINB>
+__global__ void __launch_bounds__(kNT, MINB)
     fwd_loop_kernel(const __grid_constant__ FwdLoopMaps maps, const FwdLoopArgs la) {
     using G = Geom<1, TX>;
     extern __shared__ __align__(128) float smem[];
@@ -205,56 +206,60 @@ constexpr size_t loop_smem() {
     return (size_t)S * Geom<1, TX>::STAGE * sizeof(float);
 }
 
-template <int TX, int S, bool ABC>
+template <int TX, int S, bool ABC, int B>
 cudaError_t loop_configure_one(int* ctas) {
-    auto fn = fwd_loop_kernel<TX, S, ABC>;
+    auto fn = fwd_loop_kernel<TX, S, ABC, B>;
     const size_t smem = loop_smem<TX, S>();
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, kNT, smem);
 }
 
-template <int TX, int S>
+template <int TX, int S, int B>
 cudaError_t loop_configure(int* ctas) {
     int a = 0, b = 0;
-    cudaError_t e = loop_configure_one<TX, S, true>(&a);
-    if (e == cudaSuccess) e = loop_configure_one<TX, S, false>(&b);
+    cudaError_t e = loop_configure_one<TX, S, true, B>(&a);
+    if (e == cudaSuccess) e = loop_configure_one<TX, S, false, B>(&b);
     *ctas = a < b ? a : b;
     return e;
 }
 
-template <int TX, int S>
+template <int TX, int S, int B>
 cudaError_t loop_launch(const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid, cudaStream_t st) {
     const size_t smem = loop_smem<TX, S>();
     void* args[] = {const_cast<FwdLoopMaps*>(&maps), const_cast<FwdLoopArgs*>(&la)};
     if (la.base.b1d)
-        return cudaLaunchCooperativeKernel((const void*)fwd_loop_kernel<TX, S, true>, dim3(grid), dim3(kNT), args,
+        return cudaLaunchCooperativeKernel((const void*)fwd_loop_kernel<TX, S, true, B>, dim3(grid), dim3(kNT), args,
                                            smem, st);
-    return cudaLaunchCooperativeKernel((const void*)fwd_loop_kernel<TX, S, false>, dim3(grid), dim3(kNT), args, smem,
-                                       st);
+    return cudaLaunchCooperativeKernel((const void*)fwd_loop_kernel<TX, S, false, B>, dim3(grid), dim3(kNT), args,
+                                       smem, st);
 }
 
-#define FWI_FWD_LOOP_VARIANTS(X) X(32, 2) X(16, 3) X(16, 2)
+// (tile columns, pipeline stages, CTAs per SM of the register budget).  Measured
+// on the B200: 3 CTAs per SM (70 registers) beat 2 for 16-column tiles on
+// HBM-bound surveys; 8-column tiles at 3-4 CTAs per SM lost everywhere (halo
+// overhead, a costlier grid barrier) and are not built.
+#define FWI_FWD_LOOP_VARIANTS(X) X(32, 2, 2) X(16, 3, 2) X(16, 2, 2) X(16, 2, 3)
 
 }  // namespace
 
-bool fwd_loop_supported(int TX, int S) {
-#define FWI_X(tx, s) if (TX == tx && S == s) return true;
+bool fwd_loop_supported(int TX, int S, int B) {
+#define FWI_X(tx, s, b) if (TX == tx && S == s && B == b) return true;
     FWI_FWD_LOOP_VARIANTS(FWI_X)
 #undef FWI_X
     return false;
 }
 
-cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S) {
-#define FWI_X(tx, s) if (TX == tx && S == s) return loop_configure<tx, s>(ctas_per_sm);
+cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S, int B) {
+#define FWI_X(tx, s, b) if (TX == tx && S == s && B == b) return loop_configure<tx, s, b>(ctas_per_sm);
     FWI_FWD_LOOP_VARIANTS(FWI_X)
 #undef FWI_X
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_fwd_loop(int TX, int S, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
+cudaError_t launch_fwd_loop(int TX, int S, int B, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
                             cudaStream_t st) {
-#define FWI_X(tx, s) if (TX == tx && S == s) return loop_launch<tx, s>(maps, la, grid, st);
+#define FWI_X(tx, s, b) if (TX == tx && S == s && B == b) return loop_launch<tx, s, b>(maps, la, grid, st);
     FWI_FWD_LOOP_VARIANTS(FWI_X)
 #undef FWI_X
     return cudaErrorInvalidValue;

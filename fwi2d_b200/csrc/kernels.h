@@ -35,9 +35,10 @@ struct FwdLoopMaps {
     CUtensorMap pt[4];
     CUtensorMap vel;
 };
-bool fwd_loop_supported(int TX, int S);
-cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S);
-cudaError_t launch_fwd_loop(int TX, int S, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
+// TX tile columns, S pipeline stages, B CTAs per SM the registers are budgeted for
+bool fwd_loop_supported(int TX, int S, int B);
+cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S, int B);
+cudaError_t launch_fwd_loop(int TX, int S, int B, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
                             cudaStream_t st);
 
 // ---- k_bwd_loop.cu -------------------------------------------------------------
