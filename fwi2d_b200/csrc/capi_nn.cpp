@@ -16,8 +16,25 @@ extern "C" {
 int fwi_nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
                    int relu, void* out_bf16, float* out_f32, void* stream) {
     if (!in || !w || (!out_bf16 && !out_f32) || !dims_ok(N, H, W)) return FWI_ERR_ARG;
-    if (fwi::nn_conv3x3(in, N, H, W, Cin, w, bias, Cout, relu, out_bf16, out_f32, S(stream)) != 0) return FWI_ERR_ARG;
+    const int rc = fwi::nn_conv3x3_tc(in, N, H, W, Cin, w, bias, Cout, relu, out_bf16, out_f32, S(stream));
+    if (rc == -1) return FWI_ERR_ARG;
+    if (rc != 0) return FWI_ERR_CUDA;
     return status();
+}
+
+int fwi_nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
+                       int relu, void* out_bf16, float* out_f32, void* stream) {
+    if (!in || !w || (!out_bf16 && !out_f32) || !dims_ok(N, H, W)) return FWI_ERR_ARG;
+    if (fwi::nn_conv3x3_mma(in, N, H, W, Cin, w, bias, Cout, relu, out_bf16, out_f32, S(stream)) != 0)
+        return FWI_ERR_ARG;
+    return status();
+}
+
+int fwi_nn_check(void) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return FWI_ERR_CUDA;
+    const int e = fwi::nn_tc_error(true);
+    if (e < 0) return FWI_ERR_CUDA;
+    return e ? FWI_ERR_TIMEOUT : FWI_OK;
 }
 
 size_t fwi_nn_wgrad_partial_floats(int N, int H, int W, int Cin, int Cout) {

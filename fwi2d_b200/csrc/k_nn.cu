@@ -401,8 +401,8 @@ unsigned grid_n(size_t n) {
 
 }  // namespace
 
-int nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
-               void* out, float* out32, cudaStream_t st) {
+int nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
+                   int relu, void* out, float* out32, cudaStream_t st) {
     if (Cin % 16 || Cout % 16 || N < 1 || H < 1 || W < 1) return -1;
     const int runs = (W + 15) / 16;
     const int xb = (runs + kWarps - 1) / kWarps;

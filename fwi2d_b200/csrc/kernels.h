@@ -123,8 +123,14 @@ void launch_smooth_slowness(const float* vp, int nz, int nx, const double* weigh
                             float* tmp, float* out, cudaStream_t st);
 
 // ---- k_nn.cu (CNN preconditioner; bf16 buffers passed as void*) ----------------
-int  nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
-                void* out, float* out32, cudaStream_t st);
+// tcgen05 / TMEM implicit GEMM (k_nn_tc.cu): Cin, Cout multiples of 16, <= 256
+int  nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
+                   void* out, float* out32, cudaStream_t st);
+// 1 when a bounded wait of the tcgen05 convolution gave up since the last reset
+int  nn_tc_error(bool reset);
+// mma.sync m16n8k16 implicit GEMM (k_nn.cu)
+int  nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
+                    int relu, void* out, float* out32, cudaStream_t st);
 int  nn_wgrad_chunks(long long P);
 int  nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
                       float* dw, float* db, cudaStream_t st);

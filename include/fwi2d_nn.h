@@ -25,11 +25,18 @@ extern "C" {
 
 /* out[p, co] = act(bias[co] + sum_{tap, ci} in[p + tap, ci] w[co, tap, ci]);
  * act = ReLU when relu != 0.  out_bf16 and/or out_f32 ([N,H,W,Cout]) may be
- * NULL; bias may be NULL.  Cin, Cout multiples of 16.  The data gradient of a
- * convolution is this call on the output gradient with wt of
- * fwi_nn_weight_prep, Cin and Cout swapped. */
+ * NULL; bias may be NULL.  Cin, Cout multiples of 16, at most 256.  The data
+ * gradient of a convolution is this call on the output gradient with wt of
+ * fwi_nn_weight_prep, Cin and Cout swapped.  Runs on the tcgen05 tensor cores
+ * with the accumulator in tensor memory; fwi_nn_conv3x3_mma computes the same
+ * on the mma.sync path (the first implementation, kept for comparison). */
 int fwi_nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
                    int relu, void* out_bf16, float* out_f32, void* stream);
+int fwi_nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
+                       int relu, void* out_bf16, float* out_f32, void* stream);
+/* Synchronises the device; FWI_ERR_TIMEOUT when a bounded wait inside a
+ * tcgen05 convolution gave up since the last call (the flag is then reset). */
+int fwi_nn_check(void);
 /* dw[co, tap, ci] = sum_p dout[p, co] in[p + tap, ci]; db[co] = sum_p dout[p, co]
  * (db may be NULL).  partial: fwi_nn_wgrad_partial_floats(...) floats of
  * scratch; the sums are in a fixed order (deterministic). */

@@ -260,3 +260,22 @@ def test_training_reduces_loss():
         net.adam(lr=3e-3)
         losses.append(float(net.loss.item()))
     assert losses[-1] < 0.3 * losses[0], losses[::10]
+
+
+@pytest.mark.parametrize("N,H,W,Cin,Cout", [(1, 7, 300, 16, 16), (2, 13, 29, 192, 64), (1, 9, 40, 64, 192),
+                                            (1, 5, 130, 128, 128)])
+def test_tcgen05_and_mma_sync_paths_agree(N, H, W, Cin, Cout):
+    """The tcgen05 / TMEM convolution (fwi_nn_conv3x3) and the mma.sync one
+    (fwi_nn_conv3x3_mma) give the same float32 sums up to summation order."""
+    g = torch.Generator().manual_seed(Cin + Cout)
+    x = torch.randn(N * H * W * Cin, generator=g).cuda().to(torch.bfloat16)
+    w = (torch.randn(Cout * 9 * Cin, generator=g) * 0.1).cuda().to(torch.bfloat16)
+    b = torch.randn(Cout, generator=g).cuda()
+    outs = []
+    L = api.lib()
+    for fn in (L.fwi_nn_conv3x3, L.fwi_nn_conv3x3_mma):
+        o = torch.empty(N * H * W * Cout, dtype=torch.float32, device="cuda")
+        assert fn(x.data_ptr(), N, H, W, Cin, w.data_ptr(), b.data_ptr(), Cout, 1, None, o.data_ptr(), None) == 0
+        outs.append(o)
+    assert L.fwi_nn_check() == 0
+    assert rel(outs[0], outs[1]) < 1e-5
