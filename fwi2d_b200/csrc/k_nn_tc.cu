@@ -199,13 +199,6 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
 int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
                   void* out, float* out32, cudaStream_t st) {
     if (Cin % 16 || Cin > 256 || Cout % 16 || Cout > 256 || N < 1 || H < 1 || W < 1) return -1;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) !=
-            cudaSuccess)
-            return -2;
-        configured = true;
-    }
     int ncols = 32;
     while (ncols < Cout) ncols *= 2;
     const uint32_t stage = ((uint32_t)(kTcM * Cin + Cout * Cin) * 2u + 1023u) / 1024u * 1024u;
@@ -214,6 +207,18 @@ int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, c
     size_t smem = 2 * (size_t)stage;
     const size_t tmem_share = (size_t)ncols * 460;
     if (smem < tmem_share) smem = tmem_share;
+    // dynamic shared memory above the default needs the attribute (the
+    // static 1 KB of barriers and alignment comes on top of it)
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, conv3x3_tc_kernel) != cudaSuccess) return -2;
+        if (smem + fa.sharedSizeBytes > 227 * 1024) return -1;  // two stages do not fit: unsupported size
+        if (cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -2;
+        configured = smem;
+    }
     const long long P = (long long)N * H * W;
     const unsigned grid = (unsigned)((P + kTcM - 1) / kTcM);
     conv3x3_tc_kernel<<<grid, kTcThreads, smem, st>>>(
