@@ -205,6 +205,22 @@ def profile_case(which: str = "large"):
     fields ~630 MB > L2.  small: the benchmark survey once (L2-resident)."""
     from fwi2d_b200 import api, synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_prof_"))
+    if which == "unet":
+        # the CNN preconditioner on one 301x1701 image: forward, MSE, backward
+        import torch
+        from fwi2d_b200 import cnn
+        net = cnn.UNet(seed=0)
+        H, W = 1701, 301
+        x = torch.zeros(H * W * 16, dtype=torch.bfloat16, device="cuda")
+        x.view(-1, 16)[:, :3] = torch.randn(H * W, 3, device="cuda").to(torch.bfloat16)
+        t = torch.randn(H * W, device="cuda")
+        for _ in range(2):
+            net.forward(x, 1, H, W)
+            net.mse(t)
+            net.backward(x, net.dout)
+        torch.cuda.synchronize()
+        print("profile case done: unet", float(net.loss.item()))
+        return
     if which == "batched":
         # 60 of the 240 windowed shots (every 4th), nt 40: one RTM = one
         # forward and one backward multi-level launch, fields ~1.9 GB > L2
@@ -267,7 +283,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-survey companion measurement")
-    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small", "batched"],
+    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small", "batched", "unet"],
                     help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
                          "time axis; small: the benchmark survey)")
     args = ap.parse_args()
