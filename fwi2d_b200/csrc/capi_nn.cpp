@@ -44,7 +44,17 @@ size_t fwi_nn_wgrad_partial_floats(int N, int H, int W, int Cin, int Cout) {
 int fwi_nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
                          float* dw, float* db, void* stream) {
     if (!in || !dout || !partial || !dw || !dims_ok(N, H, W)) return FWI_ERR_ARG;
-    if (fwi::nn_conv3x3_wgrad(in, dout, N, H, W, Cin, Cout, partial, dw, db, S(stream)) != 0) return FWI_ERR_ARG;
+    const int rc = fwi::nn_conv3x3_wgrad(in, dout, N, H, W, Cin, Cout, partial, dw, db, S(stream), true);
+    if (rc == -1) return FWI_ERR_ARG;
+    if (rc != 0) return FWI_ERR_CUDA;
+    return status();
+}
+
+int fwi_nn_conv3x3_wgrad_mma(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
+                             float* dw, float* db, void* stream) {
+    if (!in || !dout || !partial || !dw || !dims_ok(N, H, W)) return FWI_ERR_ARG;
+    if (fwi::nn_conv3x3_wgrad(in, dout, N, H, W, Cin, Cout, partial, dw, db, S(stream), false) != 0)
+        return FWI_ERR_ARG;
     return status();
 }
 

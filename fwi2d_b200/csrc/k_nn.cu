@@ -425,19 +425,26 @@ int nn_wgrad_chunks(long long P) {
 }
 
 int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
-                     float* dw, float* db, cudaStream_t st) {
+                     float* dw, float* db, cudaStream_t st, bool tensor_memory) {
     if (Cin % 16 || Cout % 16) return -1;
     const long long P = (long long)N * H * W;
     const int chunks = nn_wgrad_chunks(P);
     const int chunk = (int)(((P + chunks - 1) / chunks + 15) / 16 * 16);
     const auto* i16 = static_cast<const __nv_bfloat16*>(in);
     const auto* d16 = static_cast<const __nv_bfloat16*>(dout);
-    if (Cin % 32 == 0) {
-        dim3 grid(chunks, 9, (Cout / 16) * (Cin / 32));
-        wgrad_kernel<4><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
-    } else {
-        dim3 grid(chunks, 9, (Cout / 16) * (Cin / 16));
-        wgrad_kernel<2><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+    // the tcgen05 kernel takes up to 128 output channels; wider layers, and
+    // callers asking for the mma.sync path, use the warp-level kernel
+    const int tc = (tensor_memory && Cout <= 128) ? nn_wgrad_tc(in, dout, N, H, W, Cin, Cout, chunks, chunk, partial, st)
+                                                  : -1;
+    if (tc == -2) return -2;
+    if (tc != 0) {
+        if (Cin % 32 == 0) {
+            dim3 grid(chunks, 9, (Cout / 16) * (Cin / 32));
+            wgrad_kernel<4><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+        } else {
+            dim3 grid(chunks, 9, (Cout / 16) * (Cin / 16));
+            wgrad_kernel<2><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+        }
     }
     const size_t nw = (size_t)Cout * 9 * Cin;
     wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, chunks, nw, dw);

@@ -194,7 +194,145 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
     }
 }
 
+// Weight gradient of the same convolution on the tensor cores:
+//   dW[co, tap, ci] = sum_p dout[p, co] in[p + tap, ci]
+// a GEMM with M = co (padded to 128), N = ci, K = pixels.  Both operands are
+// MN-major in memory (NHWC: channels contiguous for a pixel), so they are
+// staged in the canonical MN-major layout without swizzle: core matrices of
+// 8 pixels (K rows) x 16 bytes (8 channels); K-adjacent core matrices 128 B
+// apart, channel-adjacent ones 1024 B apart (8 K groups = 64 pixels per
+// stage).  CTA (chunk, tap) accumulates its pixel chunk in TMEM and writes
+// the float32 partial[chunk][co][tap][ci]; chunks are summed in a fixed order
+// afterwards (wgrad_reduce_kernel in k_nn.cu).
+constexpr int kWgK = 64;  // pixels per stage
+
+__global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                              const __nv_bfloat16* __restrict__ dout, int N, int H,
+                                                              int W, int Cin, int Cout, int chunk, int ncols,
+                                                              uint32_t stage_bytes, float* __restrict__ partial) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tap = blockIdx.y;
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const long long P = (long long)N * H * W;
+    const long long p_begin = (long long)blockIdx.x * chunk;
+    const long long p_end = p_begin + chunk < P ? p_begin + chunk : P;
+    const uint32_t a_bytes = 16u * 8u * 128u;  // 128 co x 64 pixels
+    const int nci = Cin / 8;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_slot)),
+                     "r"(ncols)
+                     : "memory");
+        tc_fence_before();
+    }
+    if (tid == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    // M = 128, N = Cin, both operands MN-major (bits 15 and 16)
+    const uint32_t idesc = umma_idesc(128, Cin) | (1u << 15) | (1u << 16);
+    const int nstage = p_end > p_begin ? (int)((p_end - p_begin + kWgK - 1) / kWgK) : 0;
+    bool ok = true;
+    for (int st = 0; st < nstage; ++st) {
+        const int s = st & 1;
+        unsigned char* A = smem + (size_t)s * stage_bytes;
+        unsigned char* B = A + a_bytes;
+        if (st >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((st - 2) >> 1) & 1))) ok = false;
+        const long long q0 = p_begin + (long long)st * kWgK;
+        // A: dout rows (pixels) x co, 16 co groups x 64 pixels
+        for (int e = tid; e < 16 * kWgK; e += kTcThreads) {
+            const int mi = e / kWgK, r = e - mi * kWgK;  // co group, pixel in stage
+            const long long q = q0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (q < p_end && mi * 8 < Cout) v = __ldg(reinterpret_cast<const uint4*>(dout + q * Cout + mi * 8));
+            *reinterpret_cast<uint4*>(A + ((size_t)mi * 8 + (r >> 3)) * 128 + (r & 7) * 16) = v;
+        }
+        // B: shifted input rows (pixels) x ci
+        for (int e = tid; e < nci * kWgK; e += kTcThreads) {
+            const int ni = e / kWgK, r = e - ni * kWgK;
+            const long long q = q0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (q < p_end) {
+                const int x = (int)(q % W);
+                const int y = (int)((q / W) % H);
+                if (x + dx >= 0 && x + dx < W && y + dy >= 0 && y + dy < H)
+                    v = __ldg(reinterpret_cast<const uint4*>(in + (q + (long long)dy * W + dx) * Cin + ni * 8));
+            }
+            *reinterpret_cast<uint4*>(B + ((size_t)ni * 8 + (r >> 3)) * 128 + (r & 7) * 16) = v;
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sa = saddr(A), sb = saddr(B);
+            for (int k = 0; k < kWgK / 16; ++k)
+                umma_bf16(tmem, umma_desc(sa + 256u * k, 128u, 1024u), umma_desc(sb + 256u * k, 128u, 1024u), idesc,
+                          (st | k) != 0 ? 1u : 0u);
+            umma_commit(&bar[s]);
+        }
+    }
+    // collect the last use of each stage
+    for (int s = 0; s < 2; ++s) {
+        const int last = nstage - 1 - ((nstage - 1 - s) & 1);  // last stage index with parity s
+        if (last >= 0 && last % 2 == s && !tma::mbar_wait(&bar[s], (uint32_t)((last >> 1) & 1))) ok = false;
+    }
+    tc_fence_after();
+    const int co = tid;  // TMEM lane = output channel
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < Cin; c0 += 8) {
+        uint32_t r[8];
+        tmem_ld8(lane_addr + (uint32_t)c0, r);
+        if (co >= Cout) continue;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = nstage > 0 ? __uint_as_float(r[j]) : 0.0f;
+        float4* o = reinterpret_cast<float4*>(partial + (((size_t)blockIdx.x * Cout + co) * 9 + tap) * Cin + c0);
+        o[0] = make_float4(v[0], v[1], v[2], v[3]);
+        o[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    if (!ok) atomicExch(&g_tc_err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+}
+
 }  // namespace
+
+int nn_wgrad_tc(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, int chunks, int chunk,
+                float* partial, cudaStream_t st) {
+    if (Cin % 16 || Cin > 256 || Cout % 16 || Cout > 128 || chunks < 1 || chunk % 16) return -1;
+    int ncols = 32;
+    while (ncols < Cin) ncols *= 2;
+    const uint32_t stage = 16u * 8u * 128u + (uint32_t)Cin * 128u;
+    size_t smem = 2 * (size_t)stage;
+    const size_t tmem_share = (size_t)ncols * 460;
+    if (smem < tmem_share) smem = tmem_share;
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, wgrad_tc_kernel) != cudaSuccess) return -2;
+        if (smem + fa.sharedSizeBytes > 227 * 1024) return -1;
+        if (cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -2;
+        configured = smem;
+    }
+    wgrad_tc_kernel<<<dim3(chunks, 9), kTcThreads, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
+                                                               static_cast<const __nv_bfloat16*>(dout), N, H, W, Cin,
+                                                               Cout, chunk, ncols, stage, partial);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
                   void* out, float* out32, cudaStream_t st) {

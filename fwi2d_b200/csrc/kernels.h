@@ -132,8 +132,11 @@ int  nn_tc_error(bool reset);
 int  nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
                     int relu, void* out, float* out32, cudaStream_t st);
 int  nn_wgrad_chunks(long long P);
+// tensor_memory: chunk partials on the tcgen05 kernel (Cout <= 128), else mma.sync
 int  nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
-                      float* dw, float* db, cudaStream_t st);
+                      float* dw, float* db, cudaStream_t st, bool tensor_memory = true);
+int  nn_wgrad_tc(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, int chunks, int chunk,
+                 float* partial, cudaStream_t st);
 void nn_weight_prep(const float* w, int Cout, int Cin, void* wb, void* wt, cudaStream_t st);
 void nn_pool_fwd(const void* in, int N, int H, int W, int C, void* out, cudaStream_t st);
 void nn_pool_bwd(const float* dout, int N, int H, int W, int C, float* din, int accumulate, cudaStream_t st);

@@ -279,3 +279,30 @@ def test_tcgen05_and_mma_sync_paths_agree(N, H, W, Cin, Cout):
         outs.append(o)
     assert L.fwi_nn_check() == 0
     assert rel(outs[0], outs[1]) < 1e-5
+
+
+@pytest.mark.parametrize("N,H,W,Cin,Cout", [(1, 7, 300, 16, 16), (2, 13, 29, 192, 64), (1, 9, 40, 48, 16),
+                                            (3, 5, 130, 128, 128), (1, 11, 17, 96, 32)])
+def test_tcgen05_and_mma_sync_weight_gradients_agree(N, H, W, Cin, Cout):
+    """fwi_nn_conv3x3_wgrad (tcgen05 partials) and fwi_nn_conv3x3_wgrad_mma
+    (mma.sync partials) give the same weight and bias gradients."""
+    g = torch.Generator().manual_seed(7 * Cin + Cout)
+    x = torch.randn(N * H * W * Cin, generator=g).cuda().to(torch.bfloat16)
+    dy = torch.randn(N * H * W * Cout, generator=g).cuda().to(torch.bfloat16)
+    L = api.lib()
+    part = torch.empty(L.fwi_nn_wgrad_partial_floats(N, H, W, Cin, Cout), dtype=torch.float32, device="cuda")
+    res = []
+    for fn in (L.fwi_nn_conv3x3_wgrad, L.fwi_nn_conv3x3_wgrad_mma):
+        dw = torch.empty(Cout * 9 * Cin, dtype=torch.float32, device="cuda")
+        db = torch.empty(Cout, dtype=torch.float32, device="cuda")
+        assert fn(x.data_ptr(), dy.data_ptr(), N, H, W, Cin, Cout, part.data_ptr(), dw.data_ptr(), db.data_ptr(),
+                  None) == 0
+        res.append((dw, db))
+    assert L.fwi_nn_check() == 0
+    assert rel(res[0][0], res[1][0]) < 1e-5
+    assert torch.equal(res[0][1], res[1][1])
+    # and both against torch
+    xr = nhwc_to_nchw(x.float().cpu(), N, H, W, Cin)
+    dyr = nhwc_to_nchw(dy.float().cpu(), N, H, W, Cout)
+    ref = torch.nn.grad.conv2d_weight(xr, (Cout, Cin, 3, 3), dyr, padding=1)
+    assert rel(w_to_torch(res[0][0].cpu(), Cout, Cin), ref) < 1e-5
