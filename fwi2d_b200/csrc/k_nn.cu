@@ -198,6 +198,27 @@ __global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dout, long lo
     if (threadIdx.x == 0) db[co] = red[0];
 }
 
+// Bias gradient per pixel chunk: thread t sums channel t % Cout over every
+// (256 / Cout)-th pixel of the chunk (coalesced rows), the lanes of a channel
+// are added in lane order; partial[chunk][co].  Cout divides 256.
+__global__ void bias_partial_kernel(const __nv_bfloat16* __restrict__ dout, long long P, int Cout, int chunk,
+                                    float* __restrict__ partial) {
+    __shared__ float red[256];
+    const int lanes = 256 / Cout;
+    const int co = threadIdx.x % Cout, lane = threadIdx.x / Cout;
+    const long long p0 = (long long)blockIdx.x * chunk;
+    const long long p1 = p0 + chunk < P ? p0 + chunk : P;
+    float sum = 0.0f;
+    for (long long p = p0 + lane; p < p1; p += lanes) sum += __bfloat162float(dout[p * Cout + co]);
+    red[threadIdx.x] = sum;
+    __syncthreads();
+    if (lane == 0) {
+        float t = 0.0f;
+        for (int l = 0; l < lanes; ++l) t += red[l * Cout + co];
+        partial[(size_t)blockIdx.x * Cout + co] = t;
+    }
+}
+
 // bf16 weights and the data-gradient weights wT[ci][8-tap][co] from the
 // float32 master copy w[co][tap][ci]
 __global__ void weight_prep_kernel(const float* __restrict__ w, int Cout, int Cin, __nv_bfloat16* __restrict__ wb,
@@ -448,7 +469,14 @@ int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int 
     }
     const size_t nw = (size_t)Cout * 9 * Cin;
     wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, chunks, nw, dw);
-    if (db) bias_grad_kernel<<<Cout, 256, 0, st>>>(d16, P, Cout, db);
+    if (db) {
+        if (256 % Cout == 0) {  // the chunk partials are consumed: reuse the scratch
+            bias_partial_kernel<<<chunks, 256, 0, st>>>(d16, P, Cout, chunk, partial);
+            wgrad_reduce_kernel<<<grid_n((size_t)Cout), 256, 0, st>>>(partial, chunks, (size_t)Cout, db);
+        } else {
+            bias_grad_kernel<<<Cout, 256, 0, st>>>(d16, P, Cout, db);
+        }
+    }
     return 0;
 }
 
