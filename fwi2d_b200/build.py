@@ -35,6 +35,7 @@ CU_SOURCES = {
     "k_stencil.cu": [],
     "k_fwd_tma.cu": [],
     "k_fwd_loop.cu": [],
+    "k_fwd_res.cu": [],
     "k_bwd_loop.cu": [],
     "k_prep.cu": ["-fmad=false"],
     "k_nn.cu": [],
@@ -48,7 +49,8 @@ APPS = ["modeling", "migration", "inversion"]
 
 
 def _headers() -> list[Path]:
-    return list(CSRC.glob("*.h")) + list(CSRC.glob("*.hpp")) + [ROOT / "include" / "fwi2d.h"]
+    return (list(CSRC.glob("*.h")) + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh"))
+            + [ROOT / "include" / "fwi2d.h"])
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

@@ -211,6 +211,8 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
     up(&t->d_rec_colptr, rec_colptr, "receiver columns");
     up(&t->d_rec_z, rec_z, "receiver rows");
     up(&t->d_rec_soff, rec_soff, "receiver offsets");
+    t->h_src_colptr = std::move(src_colptr);
+    t->h_rec_colptr = std::move(rec_colptr);
 }
 
 void Engine::free_tables(Tables* t) {
@@ -346,7 +348,7 @@ Engine::~Engine() {
                     d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
                     d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_, d_sync_,
-                    d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_};
+                    d_slabs_, d_xbuf_, d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& r : timed_) {
@@ -704,6 +706,8 @@ double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables&
     if (p.kind == 2) {
         upload_tile_base(g, ns, p.cfg.TX);
         launch_fwd_loop_levels(p, g, t, ns, vel, vel_stride, abc, false, nullptr, 0, 2);  // warm-up
+    } else if (p.kind == 3) {
+        launch_fwd_res_levels(p, g, t, vel, vel_stride, abc, nullptr, fld_[0], fld_[1], fld_[2], fld_[3], 0, 2);
     } else {
         one(0);  // first use: module load, tensor maps
     }
@@ -714,6 +718,9 @@ double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables&
     for (int rep = 0; rep < 2; ++rep) {  // best of two timed runs
         check(cudaEventRecord(e0, st_), "event record");
         if (p.kind == 2) launch_fwd_loop_levels(p, g, t, ns, vel, vel_stride, abc, false, nullptr, 0, loop_steps);
+        else if (p.kind == 3)
+            launch_fwd_res_levels(p, g, t, vel, vel_stride, abc, nullptr, fld_[0], fld_[1], fld_[2], fld_[3], 0,
+                                  loop_steps);
         else
             for (int k = 0; k < reps; ++k) one(k);
         check(cudaEventRecord(e1, st_), "event record");
@@ -724,7 +731,7 @@ double Engine::time_fwd_candidate(const FwdPlan& p, const Grid& g, const Tables&
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const int steps = p.kind == 2 ? loop_steps : reps * (p.kind == 1 ? p.cfg.T : 1);
+    const int steps = p.kind >= 2 ? loop_steps : reps * (p.kind == 1 ? p.cfg.T : 1);
     return 1e3 * ms / steps;
 }
 
@@ -778,6 +785,136 @@ void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Table
     ++launches_;
 }
 
+bool Engine::plan_resident(const Grid& g, const Tables& t, int ns, FwdPlan* p) {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const size_t static_smem = fwd_res_static_smem();
+    if ((size_t)optin <= static_smem) return false;
+    const size_t max_dyn = (size_t)optin - static_smem;
+    const int qg = g.ldz / 4;
+    const int wcap = (int)(max_dyn / (8 * (size_t)(g.ldz + 8))) - 8;  // two buffers of (w + 8) columns
+    std::vector<int> nxx(ns);
+    for (int s = 0; s < ns; ++s) nxx[s] = h_shot_nxx(g, s);
+    // slabs of at most W columns: per shot n slabs of equal width (a multiple
+    // of 4, so that the edge runs are whole), the last taking the rest
+    std::vector<ResSlab> slabs;
+    int wmax = 0;
+    auto build = [&](int W) {
+        slabs.clear();
+        wmax = 0;
+        for (int s = 0; s < ns; ++s) {
+            const int n = (nxx[s] + W - 1) / W;
+            const int base = ((nxx[s] + n - 1) / n + 3) / 4 * 4;
+            std::vector<int> w(n, base);
+            w[n - 1] = nxx[s] - (n - 1) * base;
+            if (n > 1 && w[n - 1] < 4) {
+                w[n - 2] -= 4;
+                w[n - 1] += 4;
+            }
+            const int first = (int)slabs.size();
+            const ShotDesc& sd = t.shots[batch_s0_ + s];
+            int x0 = 0;
+            for (int k = 0; k < n; ++k) {
+                if (w[k] < 4) return false;
+                ResSlab sl{};
+                sl.s = s;
+                sl.x0 = x0;
+                sl.w = w[k];
+                sl.left = k > 0 ? first + k - 1 : -1;
+                sl.right = k + 1 < n ? first + k + 1 : -1;
+                const int a = sd.col_off + x0, b = sd.col_off + x0 + w[k];
+                if (t.h_rec_colptr[b] - t.h_rec_colptr[a] > fwd_res_max_rec()) return false;
+                if (t.h_src_colptr[b] - t.h_src_colptr[a] > fwd_res_max_src()) return false;
+                slabs.push_back(sl);
+                x0 += w[k];
+                wmax = std::max(wmax, w[k]);
+            }
+        }
+        return true;
+    };
+    // the narrowest slab width whose slabs fit one per SM
+    bool found = false;
+    for (int W = 4; W <= wcap && !found; W += 4) {
+        long long total = 0;
+        for (int s = 0; s < ns; ++s) total += (nxx[s] + W - 1) / W;
+        found = total <= sm_count_ && build(W);
+    }
+    if (!found) return false;
+    const long long items = (long long)((wmax + 3) / 4) * qg;
+    const int ipt = (int)((items + fwd_res_threads() - 1) / fwd_res_threads());
+    const size_t smem = fwd_res_smem((wmax + 3) / 4 * 4, g.ldz);
+    if (!fwd_res_fits(wmax, g.ldz) || smem > max_dyn) return false;
+    int ctas = 0;
+    if (fwd_res_configure(smem, &ctas) != cudaSuccess || ctas < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    if ((long long)slabs.size() > (long long)sm_count_ * ctas) return false;
+    p->ipt = ipt;
+    p->wmax = (wmax + 3) / 4 * 4;  // buffer columns: whole 4-column runs
+    p->smem = smem;
+    p->grid = (int)slabs.size();
+    p->slabs = std::move(slabs);
+    return true;
+}
+
+void Engine::launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables& t, const float* vel,
+                                   long long vel_stride, bool abc, float* d_seis, const float* in_cur,
+                                   const float* in_old, float* out_cur, float* out_old, int t_begin, int t_end,
+                                   long long timed_updates) {
+    const size_t nsl = p.slabs.size();
+    const size_t xb = (size_t)8 * nsl * g.ldz;  // 16-byte words: 2 parities x 2 sides x 2 ldz per slab
+    if (nsl > slabs_cap_ || xb > xbuf_cap_) {
+        check(cudaStreamSynchronize(st_), "sync before resident-kernel tables");
+        cudaFree(d_slabs_);
+        cudaFree(d_xbuf_);
+        d_slabs_ = nullptr;
+        d_xbuf_ = nullptr;
+        slabs_cap_ = std::max(slabs_cap_, nsl);
+        xbuf_cap_ = std::max(xbuf_cap_, xb);
+        d_slabs_ = dalloc<ResSlab>(slabs_cap_, "slab table");
+        d_xbuf_ = dalloc<uint4>(xbuf_cap_, "halo exchange buffer");
+    }
+    check(cudaMemcpyAsync(d_slabs_, p.slabs.data(), nsl * sizeof(ResSlab), cudaMemcpyHostToDevice, st_),
+          "upload slab table");
+    FwdResArgs a;
+    a.shots = d_batch_;
+    a.slabs = d_slabs_;
+    a.nslab = (int)nsl;
+    a.wmax = p.wmax;
+    a.ldz = g.ldz;
+    a.nzz = g.nzz;
+    a.nb = g.nb;
+    a.fstride = g.fstride();
+    a.vel = vel;
+    a.vel_stride = vel_stride;
+    a.dt2idh2 = dt_ * dt_ * idh2_;
+    a.b1d = abc ? d_b1d_ : nullptr;
+    a.inj = InjTable{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, -1, idh2_};
+    a.rec = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, nullptr, -1, 0.0f};
+    a.seis = d_seis;
+    a.t_begin = t_begin;
+    a.t_end = t_end;
+    a.nt = nt_;
+    a.tlag = tlag_;
+    a.in_cur = in_cur;
+    a.in_old = in_old;
+    a.out_cur = out_cur;
+    a.out_old = out_old;
+    a.xbuf = d_xbuf_;
+    a.err = d_err_;
+    check(cudaMemsetAsync(d_xbuf_, 0, xb * sizeof(uint4), st_), "memset halo exchange buffer");
+    TimedRegion r;
+    if (timed_updates >= 0) timing_begin(&r);
+    check(launch_fwd_res(a, p.smem, st_), "resident forward launch");
+    if (timed_updates >= 0) timing_end(&r, 1, timed_updates);
+    ++launches_;
+}
+
 Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool abc, const float* vel,
                                  long long vel_stride) {
     const long long key = ((long long)(&g == &abc_ ? 0 : 1) * 2 + (abc ? 1 : 0)) * 4 * 1000000LL +
@@ -818,8 +955,18 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         p.grid = sm_count_ * ctas;
         return p;
     };
+    auto make_res = [&]() {
+        FwdPlan p;
+        p.kind = 3;
+        if (!plan_resident(g, t, ns, &p)) p.kind = -1;
+        return p;
+    };
     std::vector<FwdPlan> cands;
-    if (fwd_kernel_ == "simple") {
+    if (fwd_kernel_ == "resident") {
+        cands.push_back(make_res());
+        if (cands.back().kind < 0)
+            throw Error(FWI_ERR_PARAM, "fwd_kernel 'resident': the batch's fields do not fit the SMs' shared memory");
+    } else if (fwd_kernel_ == "simple") {
         cands.push_back(FwdPlan{});
     } else if (fwd_kernel_.rfind("tma:", 0) == 0) {
         int T = 0, TX = 0, S = 0;
@@ -838,8 +985,9 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         for (const auto& v : variants) cands.push_back(make(v[0], v[1], v[2]));
         const int loops[][3] = {{32, 2, 2}, {16, 3, 2}, {16, 2, 2}, {16, 2, 3}};
         for (const auto& v : loops) cands.push_back(make_loop(v[0], v[1], v[2]));
+        cands.push_back(make_res());
     } else {
-        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma, tma:T,TX,S or loop:TX,S[,B]");
+        throw Error(FWI_ERR_PARAM, "fwd_kernel must be auto, simple, tma, tma:T,TX,S, loop:TX,S[,B] or resident");
     }
     FwdPlan best;
     double best_us = 1e30;
@@ -853,6 +1001,7 @@ Engine::FwdPlan Engine::fwd_plan(const Grid& g, const Tables& t, int ns, bool ab
         c.us_per_step = time_fwd_candidate(c, g, t, ns, vel, vel_stride, abc);
         if (c.kind == 0) log << " simple=" << c.us_per_step;
         else if (c.kind == 2) log << " loop" << c.cfg.TX << "," << c.cfg.S << "," << c.minb << "=" << c.us_per_step;
+        else if (c.kind == 3) log << " resident=" << c.us_per_step;
         else log << " tma" << c.cfg.T << "," << c.cfg.TX << "," << c.cfg.S << "=" << c.us_per_step;
         if (c.us_per_step < best_us) {
             best_us = c.us_per_step;
@@ -874,6 +1023,8 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
         if (plan.kind == 0) d << "simple";
         else if (plan.kind == 2)
             d << "loop TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " B=" << plan.minb << " grid=" << plan.grid;
+        else if (plan.kind == 3)
+            d << "resident W=" << plan.wmax << " IPT=" << plan.ipt << " grid=" << plan.grid;
         else d << "tma T=" << plan.cfg.T << " TX=" << plan.cfg.TX << " S=" << plan.cfg.S << " grid=" << plan.grid;
         if (!plan.tuning.empty()) d << " | us/step:" << plan.tuning;
         last_fwd_plan = d.str();
@@ -885,6 +1036,15 @@ void Engine::run_forward(const Grid& g, const Tables& t, int ns, const float* ve
     launch_inject_points(B[0], fs, d_batch_, ns, inj, g.ldz, st_);
     ++launches_;
     const int N = nt_ + tlag_;
+    if (plan.kind == 3) {
+        // every level in one cooperative launch, the fields resident in shared memory
+        launch_fwd_res_levels(plan, g, t, vel, vel_stride, abc, record ? d_seis : nullptr, B[0], B[1], B[2], B[3], 0,
+                              N, (long long)N * batch_points(g, ns));
+        fwd_cur_ = B[2];
+        fwd_old_ = B[3];
+        check(cudaGetLastError(), "forward propagation");
+        return;
+    }
     if (plan.kind == 2) {
         // every level in one cooperative launch: buffers rotate cur -> old, free -> cur
         upload_tile_base(g, ns, plan.cfg.TX);

@@ -118,6 +118,7 @@ private:
         int* d_rec_colptr = nullptr;       // nsrc*(nxx+1)
         int* d_rec_z = nullptr;            // nsrc*nrec, sorted by column
         long long* d_rec_soff = nullptr;
+        std::vector<int> h_src_colptr, h_rec_colptr;  // host copies of the column tables
     };
     enum Kind { kFwdRecord = 0, kFwdNoRecord = 1, kBwdImage = 2, kBwdGradient = 3 };
 
@@ -139,11 +140,14 @@ private:
     // forward-kernel choice for (grid, batch size, ABC): the simple tiled kernel
     // (k_stencil.cu) or a persistent TMA variant (k_fwd_tma.cu), autotuned
     struct FwdPlan {
-        int kind = 0;                 // 0 simple, 1 TMA (per-launch), 2 multi-level
+        int kind = 0;                 // 0 simple, 1 TMA (per-launch), 2 multi-level, 3 resident
         FwdTmaConfig cfg{1, 32, 2};
         FwdTmaConfig tail{1, 32, 2};  // T = 1 variant for an odd last step
         int grid = 0, tail_grid = 0;
         int minb = 2;                 // multi-level kernel: CTAs per SM of its register budget
+        int ipt = 0, wmax = 0;        // resident kernel: items per thread, widest slab
+        size_t smem = 0;              // resident kernel: dynamic shared memory
+        std::vector<ResSlab> slabs;   // resident kernel: one per CTA
         double us_per_step = 0;
         std::string tuning;           // autotuner timings of all candidates
     };
@@ -172,6 +176,13 @@ private:
     void launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                                 long long vel_stride, bool abc, bool record, float* d_seis, int t_begin, int t_end,
                                 long long timed_updates = -1);
+    // shared-memory-resident forward kernel (k_fwd_res.cu): slabs of the batch
+    // when its two time levels fit the SMs' shared memory
+    bool plan_resident(const Grid& g, const Tables& t, int ns, FwdPlan* p);
+    void launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables& t, const float* vel,
+                               long long vel_stride, bool abc, float* d_seis, const float* in_cur,
+                               const float* in_old, float* out_cur, float* out_old, int t_begin, int t_end,
+                               long long timed_updates = -1);
     // events of one timed forward region: begin is recorded before the
     // region's kernel(s), end after them
     struct TimedRegion {
@@ -274,6 +285,9 @@ private:
     int* d_tile_base_ = nullptr;
     int* d_err_ = nullptr;
     unsigned* d_sync_ = nullptr;       // grid-barrier counter of the multi-level kernel
+    ResSlab* d_slabs_ = nullptr;       // resident kernel: slab table and halo exchange words
+    uint4* d_xbuf_ = nullptr;
+    size_t slabs_cap_ = 0, xbuf_cap_ = 0;
     int sm_count_ = 0;
     std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S
     float* fwd_cur_ = nullptr;         // Q^N after run_forward

@@ -8,6 +8,7 @@
 // with a fixed per-shot stride (fstride = ldz * max columns).
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>
 
 namespace fwi {
 
@@ -90,6 +91,37 @@ struct FwdLoopArgs {
     int buf_cur, buf_old, buf_free;  // indices into bufs at t_begin
     float* bufs[4];
     unsigned* sync;           // grid-barrier counter, zero at launch
+};
+
+// Shared-memory-resident forward kernel (k_fwd_res.cu): CTA b owns slab b,
+// columns [x0, x0+w) of shot s over the full depth.  left / right: the CTAs
+// owning the neighbouring slabs of the same shot, -1 at the shot's edge.
+struct ResSlab {
+    int s, x0, w, left, right;
+    int pad[3];
+};
+
+struct FwdResArgs {
+    const ShotDesc* shots;
+    const ResSlab* slabs;
+    int nslab, wmax;          // CTAs (one per slab); widest slab
+    int ldz, nzz, nb;
+    long long fstride;        // per-shot stride of the field buffers
+    const float* vel;         // velocity, padded layout
+    long long vel_stride;     // per-shot stride of vel (0: shared by all shots)
+    float dt2idh2;
+    const float* b1d;         // ABC profile or NULL
+    InjTable inj;             // source table (sample set per level)
+    InjTable rec;             // receiver table (colptr, z, soff)
+    float* seis;              // trace-major seismograms, NULL when not recording
+    int t_begin, t_end, nt, tlag;
+    const float* in_cur;      // Q^t at t_begin
+    const float* in_old;      // Q^{t-1} at t_begin
+    float* out_cur;           // Q^t at t_end
+    float* out_old;           // Q^{t-1} at t_end
+    uint4* xbuf;              // halo words {v0, level, v1, level}: [2 parities][nslab][2 sides][2 ldz],
+                              // zero at launch
+    int* err;
 };
 
 struct FwdTmaConfig {

@@ -41,6 +41,16 @@ cudaError_t fwd_loop_configure(int* ctas_per_sm, int TX, int S, int B);
 cudaError_t launch_fwd_loop(int TX, int S, int B, const FwdLoopMaps& maps, const FwdLoopArgs& la, int grid,
                             cudaStream_t st);
 
+// ---- k_fwd_res.cu --------------------------------------------------------------
+int fwd_res_threads();               // compute threads per CTA
+int fwd_res_max_rec();               // receiver entries per slab
+int fwd_res_max_src();               // injection points per slab
+bool fwd_res_fits(int w, int ldz);   // a slab of w columns fits the kernel's TMEM item table
+size_t fwd_res_smem(int wmax, int ldz);  // dynamic shared memory for slabs up to wmax columns
+size_t fwd_res_static_smem();
+cudaError_t fwd_res_configure(size_t smem, int* ctas_per_sm);
+cudaError_t launch_fwd_res(const FwdResArgs& a, size_t smem, cudaStream_t st);
+
 // ---- k_bwd_loop.cu -------------------------------------------------------------
 // Tensor maps of the backward kernel: stencil boxes (128+8 rows, TX+8 columns)
 // and pointwise boxes (128 rows, TX columns), indexed like BwdLoopArgs.ps/pr.

@@ -21,14 +21,34 @@ __device__ __forceinline__ float el(const float4& v, int e) {
     return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
 }
 
+// dh^2 * Laplacian at rows r..r+3 of one column from its x window W[0..8]
+// (columns c-4..c+4 at rows r..r+3) and its z neighbours up (rows r-4..r-1)
+// and dn (rows r+4..r+7).
+__device__ __forceinline__ void lap_col(const float4* W, const float4& up, const float4& dn, float out[4]) {
+    const float k0 = (float)(-2.0 * kFDM5), k1 = (float)kFDM4, k2 = (float)(-kFDM3), k3 = (float)kFDM2,
+                k4 = (float)(-kFDM1);
+    const float4 ow = W[4];
+    const float z[12] = {up.x, up.y, up.z, up.w, ow.x, ow.y, ow.z, ow.w, dn.x, dn.y, dn.z, dn.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float s1 = (el(W[3], e) + el(W[5], e)) + (z[e + 3] + z[e + 5]);
+        const float s2 = (el(W[2], e) + el(W[6], e)) + (z[e + 2] + z[e + 6]);
+        const float s3 = (el(W[1], e) + el(W[7], e)) + (z[e + 1] + z[e + 7]);
+        const float s4 = (el(W[0], e) + el(W[8], e)) + (z[e + 0] + z[e + 8]);
+        float l = k4 * s4;
+        l = fmaf(k3, s3, l);
+        l = fmaf(k2, s2, l);
+        l = fmaf(k1, s1, l);
+        out[e] = fmaf(k0, z[e + 4], l);
+    }
+}
+
 // dh^2 * Laplacian at rows r..r+3 of the R consecutive columns c0..c0+R-1 of
 // a shared tile stored column by column (LD floats per column, rows
 // contiguous).  The R+8 float4 columns of the x stencil are read once into
 // registers.  `own` returns the centre values.
-template <int LD, int R>
-__device__ __forceinline__ void lap_run(const float* t, int r, int c0, float out[R][4], float4 own[R]) {
-    const float k0 = (float)(-2.0 * kFDM5), k1 = (float)kFDM4, k2 = (float)(-kFDM3), k3 = (float)kFDM2,
-                k4 = (float)(-kFDM1);
+template <int R>
+__device__ __forceinline__ void lap_run_ld(const float* t, int LD, int r, int c0, float out[R][4], float4 own[R]) {
     float4 W[R + 8];
 #pragma unroll
     for (int j = 0; j < R + 8; ++j) W[j] = *reinterpret_cast<const float4*>(t + (c0 - 4 + j) * LD + r);
@@ -37,22 +57,15 @@ __device__ __forceinline__ void lap_run(const float* t, int r, int c0, float out
         const float* col = t + (c0 + m) * LD + r;
         const float4 up = *reinterpret_cast<const float4*>(col - 4);
         const float4 dn = *reinterpret_cast<const float4*>(col + 4);
-        const float4 ow = W[m + 4];
-        own[m] = ow;
-        const float z[12] = {up.x, up.y, up.z, up.w, ow.x, ow.y, ow.z, ow.w, dn.x, dn.y, dn.z, dn.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float s1 = (el(W[m + 3], e) + el(W[m + 5], e)) + (z[e + 3] + z[e + 5]);
-            const float s2 = (el(W[m + 2], e) + el(W[m + 6], e)) + (z[e + 2] + z[e + 6]);
-            const float s3 = (el(W[m + 1], e) + el(W[m + 7], e)) + (z[e + 1] + z[e + 7]);
-            const float s4 = (el(W[m + 0], e) + el(W[m + 8], e)) + (z[e + 0] + z[e + 8]);
-            float l = k4 * s4;
-            l = fmaf(k3, s3, l);
-            l = fmaf(k2, s2, l);
-            l = fmaf(k1, s1, l);
-            out[m][e] = fmaf(k0, z[e + 4], l);
-        }
+        own[m] = W[m + 4];
+        lap_col(W + m, up, dn, out[m]);
     }
+}
+
+// The same with the column pitch LD known at compile time.
+template <int LD, int R>
+__device__ __forceinline__ void lap_run(const float* t, int r, int c0, float out[R][4], float4 own[R]) {
+    lap_run_ld<R>(t, LD, r, c0, out, own);
 }
 
 // Per-thread facts about its 4 rows i0..i0+3: update-region membership and
@@ -99,16 +112,21 @@ __device__ __forceinline__ float damp(const Rows& r, const Col& c, int e) {
     return ((r.inz >> e) & 1u) && c.inx ? (r.dz[e] + c.dx) - 1.0f : r.dz[e] * c.dx;
 }
 
-// One float4 of the forward update.  EDGE: apply the Dirichlet zeroing;
-// DAMP: apply the Cerjan damper.
+// The coefficient dt^2/dh^2 * v^2 of the four points, k2 * (v * v).
+__device__ __forceinline__ float4 coef4(const float4& v, float k2) {
+    return make_float4(k2 * (v.x * v.x), k2 * (v.y * v.y), k2 * (v.z * v.z), k2 * (v.w * v.w));
+}
+
+// One float4 of the forward update from the coefficients k4 = coef4(v, k2)
+// (kernels that keep them resident call this directly).  EDGE: apply the
+// Dirichlet zeroing; DAMP: apply the Cerjan damper.
 template <bool DAMP, bool EDGE>
-__device__ __forceinline__ float4 update4(const float l[4], const float4& q, const float4& o, const float4& v,
-                                          float k2, const Rows& r, const Col& c) {
+__device__ __forceinline__ float4 update4k(const float l[4], const float4& q, const float4& o, const float4& k4,
+                                           const Rows& r, const Col& c) {
     float out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const float vv = el(v, e);
-        const float kk = k2 * (vv * vv);
+        const float kk = el(k4, e);
         float res;
         if (DAMP) {
             const float d = damp(r, c, e);
@@ -120,6 +138,12 @@ __device__ __forceinline__ float4 update4(const float l[4], const float4& q, con
         out[e] = res;
     }
     return make_float4(out[0], out[1], out[2], out[3]);
+}
+
+template <bool DAMP, bool EDGE>
+__device__ __forceinline__ float4 update4(const float l[4], const float4& q, const float4& o, const float4& v,
+                                          float k2, const Rows& r, const Col& c) {
+    return update4k<DAMP, EDGE>(l, q, o, coef4(v, k2), r, c);
 }
 
 // One float4 of the backward step (cross_correlation / build_gradient,

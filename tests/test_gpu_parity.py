@@ -95,7 +95,7 @@ def test_set_model_and_cfl(case):
 
 
 VARIANTS = ["simple", "tma:1,32,2", "tma:1,32,3", "tma:1,16,3", "tma:1,16,4", "tma:2,32,2", "tma:2,16,2",
-            "tma:2,16,3", "loop:32,2", "loop:16,3", "loop:16,2", "loop:16,2,3"]
+            "tma:2,16,3", "loop:32,2", "loop:16,3", "loop:16,2", "loop:16,2,3", "resident"]
 
 
 @pytest.mark.parametrize("nt", [500, 501])  # nt + tlag odd (T = 2 ends with a one-level launch) and even
@@ -113,7 +113,7 @@ def test_forward_kernel_variants_vs_oracle(tmp_path, variant, nt):
 def test_forward_variants_agree_on_wide_grid(tmp_path):
     """Several tiles per column and per shot, receivers across tile borders."""
     outs = {}
-    for v in ("simple", "tma:1,32,2", "tma:2,16,2", "tma:2,32,2", "loop:32,2", "loop:16,3", "loop:16,2,3"):
+    for v in ("simple", "tma:1,32,2", "tma:2,16,2", "tma:2,32,2", "loop:32,2", "loop:16,3", "loop:16,2,3", "resident"):
         c, vp = synth.small_case(tmp_path / v.replace(":", "_").replace(",", "_"), nz=260, nx=300, nt=300,
                                  nshots=4, nrec=77, fwd_kernel=v)
         with api.Context(c.params, api.MODE_MODELING) as ctx:
@@ -146,7 +146,7 @@ def _rtm_data(c, vp):
 
 @pytest.mark.parametrize("variant,bwd", [("auto", "auto"), ("simple", "simple"), ("tma:2,16,2", "loop:16,3"),
                                          ("tma:1,32,2", "loop:16,2"), ("loop:16,2", "loop:8,4"),
-                                         ("loop:32,2", "loop:8,3")])
+                                         ("loop:32,2", "loop:8,3"), ("resident", "loop:8,3")])
 def test_rtm_vs_oracle(case, tmp_path, variant, bwd):
     c0, vp = case
     c, _ = synth.small_case(tmp_path, fwd_kernel=variant, bwd_kernel=bwd)

@@ -65,7 +65,7 @@ def test_windows_reported(tmp_path):
     assert got[-1] == (0, c.nx) and all(w < c.nx for _, w in got[:-1])
 
 
-@pytest.mark.parametrize("variant", ["auto", "simple", "tma:1,32,2", "tma:2,16,2", "loop:32,2", "loop:16,3"])
+@pytest.mark.parametrize("variant", ["auto", "simple", "tma:1,32,2", "tma:2,16,2", "loop:32,2", "loop:16,3", "resident"])
 def test_windowed_modeling_vs_oracle(tmp_path, variant):
     c, vp = _case(tmp_path, fwd_kernel=variant)
     with api.Context(c.params, api.MODE_MODELING) as ctx:
