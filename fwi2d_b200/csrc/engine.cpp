@@ -796,7 +796,8 @@ bool Engine::plan_resident(const Grid& g, const Tables& t, int ns, FwdPlan* p) {
     if ((size_t)optin <= static_smem) return false;
     const size_t max_dyn = (size_t)optin - static_smem;
     const int qg = g.ldz / 4;
-    const int wcap = (int)(max_dyn / (8 * (size_t)(g.ldz + 8))) - 8;  // two buffers of (w + 8) columns
+    const size_t stage = fwd_res_stage_smem(g.ldz);  // halo staging, independent of the slab width
+    const int wcap = max_dyn > stage ? (int)((max_dyn - stage) / (8 * (size_t)(g.ldz + 8))) - 8 : 0;
     std::vector<int> nxx(ns);
     for (int s = 0; s < ns; ++s) nxx[s] = h_shot_nxx(g, s);
     // slabs of at most W columns: per shot n slabs of equal width (a multiple
@@ -877,7 +878,7 @@ void Engine::launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables
         slabs_cap_ = std::max(slabs_cap_, nsl);
         xbuf_cap_ = std::max(xbuf_cap_, xb);
         d_slabs_ = dalloc<ResSlab>(slabs_cap_, "slab table");
-        d_xbuf_ = dalloc<uint4>(xbuf_cap_, "halo exchange buffer");
+        d_xbuf_ = dalloc<ulonglong2>(xbuf_cap_, "halo exchange buffer");
     }
     check(cudaMemcpyAsync(d_slabs_, p.slabs.data(), nsl * sizeof(ResSlab), cudaMemcpyHostToDevice, st_),
           "upload slab table");
@@ -907,7 +908,7 @@ void Engine::launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables
     a.out_old = out_old;
     a.xbuf = d_xbuf_;
     a.err = d_err_;
-    check(cudaMemsetAsync(d_xbuf_, 0, xb * sizeof(uint4), st_), "memset halo exchange buffer");
+    check(cudaMemsetAsync(d_xbuf_, 0, xb * sizeof(ulonglong2), st_), "memset halo exchange buffer");
     TimedRegion r;
     if (timed_updates >= 0) timing_begin(&r);
     check(launch_fwd_res(a, p.smem, st_), "resident forward launch");

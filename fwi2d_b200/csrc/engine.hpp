@@ -286,7 +286,7 @@ private:
     int* d_err_ = nullptr;
     unsigned* d_sync_ = nullptr;       // grid-barrier counter of the multi-level kernel
     ResSlab* d_slabs_ = nullptr;       // resident kernel: slab table and halo exchange words
-    uint4* d_xbuf_ = nullptr;
+    ulonglong2* d_xbuf_ = nullptr;
     size_t slabs_cap_ = 0, xbuf_cap_ = 0;
     int sm_count_ = 0;
     std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S

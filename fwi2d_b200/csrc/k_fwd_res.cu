@@ -21,22 +21,25 @@
 //     longer fits the instruction cache;
 //   * the only traffic between CTAs is the halo: 4 columns on each side per
 //     level, exchanged through a small global buffer (L2), not a grid
-//     barrier.  Each 16-byte word carries two values and, twice, the level
-//     that wrote them (the low-latency protocol of NCCL's LL transport), so
-//     the reader polls the data itself: no fence, no flag, one L2 round trip
-//     when the data is there.  A level computes the slab's interior first
-//     (it needs no halo), then the edge columns, whose threads publish their
-//     results at once; four exchange warps fetch the neighbours' edges of the
-//     level before into the halo while the twelve compute warps finish the
-//     interior, so the exchange hides behind it.
+//     barrier.  Each value travels in a 64-bit half beside the level that
+//     wrote it (the low-latency protocol of NCCL's LL transport), so the
+//     reader checks the data itself: no fence and no flag.  A level computes
+//     the slab's two edge runs first and their threads publish the results
+//     at once; then the interior, during whose last pass every thread starts
+//     asynchronous copies (cp.async, L2 -> shared memory) of its share of the
+//     neighbours' edges, published a whole interior earlier; after the pass
+//     it checks the levels and unpacks them into the halo.  The copies never
+//     stall the compute warps (loads issued to L2 by warps of their own,
+//     queued behind the compute warps' shared-memory traffic, took longer
+//     than the whole interior), and the only barrier is the one per level.
 //
 // The exchange buffer is double-buffered by level parity: a slab rewrites a
 // parity slot two levels later, after it has read its neighbours' next
 // level, which they published only after reading that slot.  It is zeroed
-// before every launch (tag 0 is no level).  Every wait is bounded
+// before every launch (level 0 is no level).  Every wait is bounded
 // (tma::kSpinLimit polls); a wait that gives up raises *err and the CTA
-// leaves the level loop (it has no asynchronous copies in flight; its TMEM
-// is released), after which its neighbours' waits run out the same way.
+// leaves the level loop (with no asynchronous copy in flight and its TMEM
+// released), after which its neighbours' waits run out the same way.
 #include <cuda_runtime.h>
 
 #include "kargs.h"
@@ -48,34 +51,37 @@ namespace fwi {
 
 namespace {
 
-constexpr int kRC = 384;        // compute threads (12 warps, 3 per SM sub-partition)
-constexpr int kRX = 128;        // exchange threads (4 warps, 1 per sub-partition)
-constexpr int kRT = kRC + kRX;
-constexpr int kXB = 6;          // exchange words in flight per exchange thread
+constexpr int kRC = 384;        // threads (12 warps, 3 per SM sub-partition)
+constexpr int kRT = kRC;
 constexpr int kRecPerThread = 2;
+constexpr int kMaxXW = 4;       // halo words per thread and level: 4 ldz <= kMaxXW * kRT
 constexpr int kMaxSrc = 16;     // injection points per slab
 
-__device__ __forceinline__ void bar_arrive(int id, int n) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-__device__ __forceinline__ void bar_sync(int id, int n) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-// Halo words {v0, tag, v1, tag}: two values of an edge column, each beside
-// the level that wrote them.  Written and polled with 16-byte volatile
-// accesses; a word counts only when both tags equal the level awaited (the
-// 8-byte halves are each written at once), so no fence or flag is needed.
-__device__ __forceinline__ void st_word(uint4* p, uint4 v) {
-    asm volatile("st.volatile.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+// Halo words: two values of an edge column, each in a 64-bit half beside the
+// level that wrote it (value bits | level << 32).  A 64-bit access is
+// single-copy atomic, so a half whose level is the one awaited holds that
+// level's value: the reader polls the data itself, with no fence and no flag.
+// Relaxed gpu-scope accesses: they reach L2 and may be pipelined.
+__device__ __forceinline__ void st_word(ulonglong2* p, float v0, float v1, unsigned tag) {
+    const unsigned long long t = (unsigned long long)tag << 32;
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(t | __float_as_uint(v0)),
+                 "l"(t | __float_as_uint(v1))
                  : "memory");
 }
-__device__ __forceinline__ uint4 ld_word(const uint4* p) {
-    uint4 v;
-    asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p)
-                 : "memory");
+__device__ __forceinline__ ulonglong2 ld_word(const ulonglong2* p) {
+    ulonglong2 v;
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ bool word_is(const ulonglong2& v, unsigned tag) {
+    return (unsigned)(v.x >> 32) == tag && (unsigned)(v.y >> 32) == tag;
+}
+// 16-byte asynchronous copy L2 -> shared memory (bypassing L1)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // Column of receiver / source entry r of a shot: colptr[col_off + x] <= r < colptr[col_off + x + 1].
@@ -89,10 +95,10 @@ __device__ __forceinline__ int entry_column(const int* colptr, int col_off, int 
 }
 
 // Work of a slab per level, in 4 x 4 items (4 rows of a 4-column run): the
-// interior runs 1..nruns-2 first — they read only the slab's own columns —
-// then the two edge runs 0 and nruns-1, which read the halo and whose results
-// the neighbours wait for.  Pass k of a compute thread holds interior item
-// tid + k*kRC (k < pint) or edge item tid + (k-pint)*kRC.
+// two edge runs 0 and nruns-1 first — they read the halo and the neighbours
+// wait for their results — then the interior runs 1..nruns-2, which read only
+// the slab's own columns.  Pass k of a thread holds edge item tid + k*kRC
+// (k < pedge) or interior item tid + (k-pedge)*kRC.
 struct Sched {
     int qg, nruns, nint, nedge, pint, pedge;
 };
@@ -111,14 +117,14 @@ __host__ __device__ __forceinline__ Sched make_sched(int w, int ldz) {
 __device__ __forceinline__ bool item_of(const Sched& sc, int tid, int k, int* c0, int* gz) {
     int i, run;
     bool valid;
-    if (k < sc.pint) {
+    if (k < sc.pedge) {
         i = tid + k * kRC;
-        valid = i < sc.nint;
-        run = valid ? 1 + i / sc.qg : 0;
-    } else {
-        i = tid + (k - sc.pint) * kRC;
         valid = i < sc.nedge;
         run = (valid && i >= sc.qg) ? sc.nruns - 1 : 0;
+    } else {
+        i = tid + (k - sc.pedge) * kRC;
+        valid = i < sc.nint;
+        run = valid ? 1 + i / sc.qg : 0;
     }
     *c0 = 4 * run;
     *gz = valid ? 4 * (i % sc.qg) : 0;
@@ -132,9 +138,9 @@ struct SrcList {
 };
 
 // ---- tensor memory: the per-point constants live there for the launch.
-// Compute warp w reaches TMEM lanes 32*(w%4)..+31; warps w, w+4 and w+8
+// Warp w reaches TMEM lanes 32*(w%4)..+31; warps w, w+4 and w+8
 // take 160 of the 512 columns each; item k of a thread takes 32 columns:
-// per item column m, its 4 coefficients dt^2/dh^2 v^2, then its 4 dampers.
+// per item column m, its 4 negated coefficients -dt^2/dh^2 v^2, then its 4 dampers.
 constexpr int kTmemCols = 512;
 constexpr int kItemCols = 32;
 constexpr int kWarpCols = 160;
@@ -178,17 +184,86 @@ __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Q^{t+1} of one 4 x 4 item, rows gz..gz+3 of slab columns c0..c0+ncol-1:
-// the Laplacian of Q^t in A column by column from the item's x window, Q^{t-1}
-// in B (pointwise, overwritten) and the item's constants kr (per column:
-// coefficients, dampers) from TMEM.  Items of an edge run also publish their
-// results to pub_a / pub_b (a side of the slab's exchange words, or NULL).  One expression serves every point: the
-// damped update of the other kernels, new = d * (kk * L + 2 q - d * old), with
-// d = 1 outside the ABC band (multiplications by 1 are exact) and d = 0 on the
-// Dirichlet rim.
+// ---- packed FP32 pairs (sm_100 FADD2 / FMUL2 / FFMA2): two IEEE float
+// operations per instruction, each rounded as its scalar form, so the pair
+// versions below give the bits of the scalar arithmetic in half the issue
+// slots.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 upk(f2 v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// dh^2 * Laplacian at rows r..r+3 of one column, as st::lap_col (the same
+// sums in the same order) on the point pairs (r, r+1) and (r+2, r+3).  z pairs
+// aligned with a float4 are A0..A5 (up, own, dn halves); the pairs straddling
+// two halves are S0..S4.
+__device__ __forceinline__ void lap_col2(const float4* W, const float4& up, const float4& dn, f2 out[2]) {
+    const f2 k0 = pk((float)(-2.0 * kFDM5), (float)(-2.0 * kFDM5)), k1 = pk((float)kFDM4, (float)kFDM4),
+             k2 = pk((float)(-kFDM3), (float)(-kFDM3)), k3 = pk((float)kFDM2, (float)kFDM2),
+             k4 = pk((float)(-kFDM1), (float)(-kFDM1));
+    const float4 ow = W[4];
+    const f2 A0 = pk(up.x, up.y), A1 = pk(up.z, up.w), A2 = pk(ow.x, ow.y), A3 = pk(ow.z, ow.w), A4 = pk(dn.x, dn.y),
+             A5 = pk(dn.z, dn.w);
+    const f2 S0 = pk(up.y, up.z), S1 = pk(up.w, ow.x), S2 = pk(ow.y, ow.z), S3 = pk(ow.w, dn.x), S4 = pk(dn.y, dn.z);
+    // z sums per pair and k = 1..4; centres
+    const f2 zs[2][4] = {{add2(S1, S2), add2(A1, A3), add2(S0, S3), add2(A0, A4)},
+                         {add2(S2, S3), add2(A2, A4), add2(S1, S4), add2(A1, A5)}};
+    const f2 ctr[2] = {A2, A3};
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        f2 sk[4];
+#pragma unroll
+        for (int k = 1; k <= 4; ++k) {
+            const f2 xm = p == 0 ? pk(W[4 - k].x, W[4 - k].y) : pk(W[4 - k].z, W[4 - k].w);
+            const f2 xp = p == 0 ? pk(W[4 + k].x, W[4 + k].y) : pk(W[4 + k].z, W[4 + k].w);
+            sk[k - 1] = add2(add2(xm, xp), zs[p][k - 1]);
+        }
+        f2 l = mul2(k4, sk[3]);
+        l = fma2(k3, sk[2], l);
+        l = fma2(k2, sk[1], l);
+        l = fma2(k1, sk[0], l);
+        out[p] = fma2(k0, ctr[p], l);
+    }
+}
+
+// Q^{t+1} of one 4 x 4 item, rows gz..gz+3 of slab columns c0..c0+3 (a
+// partial last run of a shot computes zeros past its edge, d = 0 there): the
+// Laplacian of Q^t in A column by column from the item's x window, Q^{t-1} in
+// B (pointwise, overwritten) and the item's constants kr from TMEM (per
+// column: the negated coefficients -kk, then the dampers d).  One expression
+// serves every point, the damped update of the other kernels
+//     new = d * (kk * L + 2 q - d * old)
+// with d = 1 outside the ABC band (multiplications by 1 are exact) and d = 0
+// on the Dirichlet rim.  It is evaluated on point pairs with the same
+// roundings as its scalar contraction u = fma(kk, L, 2q), new = d * fma(-d,
+// old, u): nu = fma(-kk, L, -2q) = -u and fma(d, old, nu) = -fma(-d, old, u)
+// exactly, and new = (-d) * that.  Items of an edge run also publish their
+// results to pub_a / pub_b (a side of the slab's exchange words, or NULL).
 __device__ __forceinline__ void res_item(const FwdResArgs& a, const float* A, float* B, int lds, int c0, int gz,
-                                         int ncol, bool valid, uint32_t tcol, const SrcList& src, int sample,
-                                         uint4* pub_a, uint4* pub_b, unsigned tag) {
+                                         bool valid, bool src_here, uint32_t tcol, const SrcList& src, int sample,
+                                         ulonglong2* pub_a, ulonglong2* pub_b, unsigned tag) {
     uint32_t kr[32];
     __syncwarp();
     tmem_ld32(tcol, kr);
@@ -199,23 +274,27 @@ __device__ __forceinline__ void res_item(const FwdResArgs& a, const float* A, fl
     __syncwarp();
     tmem_wait_ld32(kr);
     if (!valid) return;
+    const f2 m2 = pk(-2.0f, -2.0f), m1 = pk(-1.0f, -1.0f);
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        if (m >= ncol) break;
         const float* col = t + m * lds;
-        float l[4];
-        st::lap_col(W + m, *reinterpret_cast<const float4*>(col - 4), *reinterpret_cast<const float4*>(col + 4), l);
+        f2 l[2];
+        lap_col2(W + m, *reinterpret_cast<const float4*>(col - 4), *reinterpret_cast<const float4*>(col + 4), l);
         float* po = B + (c0 + m + 4) * lds + 4 + gz;
         const float4 oo = *reinterpret_cast<const float4*>(po);
-        float res[4];
+        float2 res[2];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float kk = __uint_as_float(kr[8 * m + e]);
-            const float d = __uint_as_float(kr[8 * m + 4 + e]);
-            res[e] = d * (kk * l[e] + 2.0f * st::el(W[m + 4], e) - d * st::el(oo, e));
+        for (int p = 0; p < 2; ++p) {
+            // -(kk L + 2 q), d old - (kk L + 2 q), then d (kk L + 2 q - d old) = -d * that
+            const f2 nkk = pk(__uint_as_float(kr[8 * m + 2 * p]), __uint_as_float(kr[8 * m + 2 * p + 1]));
+            const f2 d = pk(__uint_as_float(kr[8 * m + 4 + 2 * p]), __uint_as_float(kr[8 * m + 5 + 2 * p]));
+            const f2 q = p == 0 ? pk(W[m + 4].x, W[m + 4].y) : pk(W[m + 4].z, W[m + 4].w);
+            const f2 o = p == 0 ? pk(oo.x, oo.y) : pk(oo.z, oo.w);
+            const f2 nu = fma2(nkk, l[p], mul2(q, m2));
+            res[p] = upk(mul2(mul2(d, m1), fma2(d, o, nu)));
         }
-        float4 out = make_float4(res[0], res[1], res[2], res[3]);
-        if (sample >= 0) {
+        float4 out = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
+        if (src_here && sample >= 0) {
             for (int k = 0; k < src.n; ++k) {
                 const int dz = src.z[k] - gz;
                 if (src.lc[k] != c0 + m || dz < 0 || dz >= 4) continue;
@@ -228,16 +307,14 @@ __device__ __forceinline__ void res_item(const FwdResArgs& a, const float* A, fl
         }
         *reinterpret_cast<float4*>(po) = out;
         // an edge column: also to the neighbour, as two tagged words
-        const size_t j = (size_t)(m * a.ldz + gz) / 2;
-        const uint4 w0 = make_uint4(__float_as_uint(out.x), tag, __float_as_uint(out.y), tag);
-        const uint4 w1 = make_uint4(__float_as_uint(out.z), tag, __float_as_uint(out.w), tag);
+        const int j = m * (a.ldz >> 1) + (gz >> 1);
         if (pub_a) {
-            st_word(pub_a + j, w0);
-            st_word(pub_a + j + 1, w1);
+            st_word(pub_a + j, out.x, out.y, tag);
+            st_word(pub_a + j + 1, out.z, out.w, tag);
         }
         if (pub_b) {
-            st_word(pub_b + j, w0);
-            st_word(pub_b + j + 1, w1);
+            st_word(pub_b + j, out.x, out.y, tag);
+            st_word(pub_b + j + 1, out.z, out.w, tag);
         }
     }
 }
@@ -255,10 +332,6 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     const int qg = a.ldz / 4;   // 4-row groups per column
     const Sched sc = make_sched(sl.w, a.ldz);
     const int passes = sc.pint + sc.pedge;
-    // the exchange warps fetch the halo during the last two interior passes:
-    // the neighbours published it as the level began, so by then it has as a
-    // rule landed in L2 and one round of loads brings it, without polling
-    const int fetch_after = sc.pint > 2 ? sc.pint - 2 : 0;
     const long long so = (long long)sl.s * a.fstride;
     // the two field buffers, as offsets into smem (the Q^t / Q^{t-1} roles
     // swap every level; offsets keep every access a shared-memory one)
@@ -327,9 +400,26 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     }
     // slabs the host planned outside these tables never run (the same test on every thread)
     const bool fits = rke - rkb <= kRecPerThread * kRC && ske - skb <= kMaxSrc && passes <= kMaxPasses &&
-                      a.ldz % 2 == 0;
+                      4 * a.ldz <= kMaxXW * kRT;
     if (!fits && tid == 0) atomicExch(a.err, 1);
-    // the thread's TMEM columns: lanes of its warp quarter, its half of the columns
+    __syncthreads();  // the source list is complete
+    // this thread's halo words, w = tid + i*kRT of the 4 ldz: w < 2 ldz from the left
+    // neighbour's right side (-> columns -4..-1), the others from the right
+    // neighbour's left side (-> columns w..w+3); xdst: float offset of the two
+    // values in a field buffer, -1 for none
+    const int nw = 2 * a.ldz;  // words per side: 4 columns, 2 values a word
+    int xdst[kMaxXW];
+#pragma unroll
+    for (int i = 0; i < kMaxXW; ++i) {
+        const int w = tid + i * kRT;
+        const bool left = w < nw;
+        xdst[i] = -1;
+        if (w < 2 * nw && (left ? sl.left : sl.right) >= 0) {
+            const int v = 2 * (left ? w : w - nw), c = v / a.ldz, z = v - c * a.ldz;
+            xdst[i] = ((left ? c - 4 : sl.w + c) + 4) * lds + 4 + z;
+        }
+    }
+    // the thread's TMEM columns: lanes of its warp's quarter, its warp's third of the columns
     const uint32_t tbase = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * kWarpCols);
     if (fits && tid < kRC) {
         // the coefficients dt^2/dh^2 v^2 and dampers of the thread's items, once
@@ -339,7 +429,11 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
         for (int k = 0; k < passes; ++k) {
             int c0 = 0, gz = 0;
             const bool valid = item_of(sc, tid, k, &c0, &gz);
-            s_pos[k * kRC + tid] = (valid ? 0 : (int)0x80000000) | (c0 << 16) | gz;
+            // item position: bit 31 no item, bit 30 an injection point inside, c0 << 16 | gz
+            bool src_here = false;
+            for (int q = 0; q < src.n && q < kMaxSrc; ++q)
+                src_here |= src.lc[q] >= c0 && src.lc[q] < c0 + 4 && src.z[q] >= gz && src.z[q] < gz + 4;
+            s_pos[k * kRC + tid] = (valid ? 0 : (int)0x80000000) | (valid && src_here ? 0x40000000 : 0) | (c0 << 16) | gz;
             const st::Rows rows = st::rows_info(a.b1d, a.nb, gz, a.nzz);
             uint32_t kr[32];
 #pragma unroll
@@ -354,7 +448,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const bool ok = col_in && col.ok && ((rows.ok >> e) & 1u);
-                    kr[8 * m + e] = __float_as_uint(ok ? st::el(k4, e) : 0.0f);
+                    kr[8 * m + e] = __float_as_uint(ok ? -st::el(k4, e) : 0.0f);
                     kr[8 * m + 4 + e] = __float_as_uint(ok ? st::damp(rows, col, e) : 0.0f);
                 }
             }
@@ -365,91 +459,72 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     }
     __syncthreads();
 
+    ulonglong2* stage = reinterpret_cast<ulonglong2*>(smem + 2 * (size_t)(a.wmax + 8) * lds);
+    // the halo of the next level is fetched during the last pass
+    const int fetch_at = passes - 1 > sc.pedge ? passes - 1 : sc.pedge;
     bool done = !fits;
     for (int t = a.t_begin; t < a.t_end && !done; ++t) {
         float* A = smem + oa;  // Q^t (stencil)
         float* B = smem + ob;  // Q^{t-1}, then Q^{t+1}
-        // level L computes Q^{t+1} and publishes its edges with tag L + 1; the
-        // halo of Q^t came with tag L (from the field buffers when L = 0)
+        // level L computes Q^{t+1} and publishes its edges with tag L + 1,
+        // which the neighbours fetch into their halo during this same level
         const unsigned lv = (unsigned)(t - a.t_begin);
-        const int nw = 2 * a.ldz;  // exchange words per side: 4 columns, 2 values a word
-        if (tid < kRC) {
-            // ---------- compute warps
-            if (a.seis && t > a.tlag) {
+        const unsigned tag = lv + 1;
+        const size_t slot = tag & 1u;
+        const bool fetch = t + 1 < a.t_end;
+        if (a.seis && t > a.tlag) {
 #pragma unroll
-                for (int j = 0; j < kRecPerThread; ++j)
-                    if (rec_idx[j] >= 0) a.seis[rec_off[j] + (t - a.tlag)] = rec_d[j] * A[rec_idx[j]];
+            for (int j = 0; j < kRecPerThread; ++j)
+                if (rec_idx[j] >= 0) a.seis[rec_off[j] + (t - a.tlag)] = rec_d[j] * A[rec_idx[j]];
+        }
+        const int sample = (t + 1 < a.nt) ? t + 1 : -1;
+        ulonglong2* mine = a.xbuf + (slot * a.nslab + blockIdx.x) * 2 * nw;
+        const ulonglong2* from_left = a.xbuf + (slot * a.nslab + (sl.left >= 0 ? sl.left : 0)) * 2 * nw + nw;
+        const ulonglong2* from_right = a.xbuf + (slot * a.nslab + (sl.right >= 0 ? sl.right : 0)) * 2 * nw;
+        for (int k = 0; k <= passes; ++k) {
+            if (k == fetch_at && fetch) {
+#pragma unroll
+                for (int i = 0; i < kMaxXW; ++i) {
+                    const int w = tid + i * kRT;
+                    if (xdst[i] >= 0) cp_async16(stage + w, w < nw ? from_left + w : from_right + (w - nw));
+                }
             }
-            const int sample = (t + 1 < a.nt) ? t + 1 : -1;
-            uint4* mine = a.xbuf + ((size_t)((lv + 1) & 1u) * a.nslab + blockIdx.x) * 2 * nw;
-            for (int k = 0; k < passes; ++k) {
-                if (k == fetch_after) bar_arrive(2, kRT);  // the exchange warps may start fetching
-                if (k == sc.pint) bar_sync(1, kRT);        // the halo of Q^t is in A
-                const int pos = s_pos[k * kRC + tid];
-                const bool valid = pos >= 0;
-                const int c0 = (pos >> 16) & 0x7fff, gz = pos & 0xffff;
-                uint4* pa = (k >= sc.pint && sl.left >= 0 && c0 == 0) ? mine : nullptr;
-                uint4* pb = (k >= sc.pint && sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
-                res_item(a, A, B, lds, c0, gz, min(4, sl.w - c0), valid, tbase + kItemCols * k, src, sample, pa, pb,
-                         lv + 1);
-            }
-            if (sc.pedge == 0) bar_sync(1, kRT);
-        } else {
-            // ---------- exchange warps: the neighbours' edges of Q^t (tag L)
-            // into the halo columns of A, while the interior is computed.
-            // Word w < nw: the left neighbour's right edge -> columns -4..-1;
-            // w >= nw: the right neighbour's left edge -> columns w..w+3.
-            bar_sync(2, kRT);
-            const int x = tid - kRC;
-            const size_t slot = lv & 1u;
-            const uint4* from_left = a.xbuf + (slot * a.nslab + (sl.left >= 0 ? sl.left : 0)) * 2 * nw + nw;
-            const uint4* from_right = a.xbuf + (slot * a.nslab + (sl.right >= 0 ? sl.right : 0)) * 2 * nw;
+            if (k == passes) break;
+            const int pos = s_pos[k * kRC + tid];
+            const bool valid = pos >= 0;
+            const int c0 = (pos >> 16) & 0x3fff, gz = pos & 0xffff;
+            ulonglong2* pa = (k < sc.pedge && sl.left >= 0 && c0 == 0) ? mine : nullptr;
+            ulonglong2* pb = (k < sc.pedge && sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
+            res_item(a, A, B, lds, c0, gz, valid, (pos & 0x40000000) != 0, tbase + kItemCols * k, src, sample, pa, pb,
+                     tag);
+        }
+        if (fetch) {
+            // unpack the words this thread fetched into the halo of B (Q^{t+1});
+            // a word not yet at this level is polled from L2 (bounded)
+            cp_async_wait_all();
             bool ok = true;
-            for (int base = x; lv > 0 && base < 2 * nw && ok; base += kRX * kXB) {
-                uint4 v[kXB];
-                unsigned pending = 0;
 #pragma unroll
-                for (int i = 0; i < kXB; ++i) {
-                    const int w = base + i * kRX;
-                    const bool left = w < nw;
-                    if (w >= 2 * nw || (left ? sl.left : sl.right) < 0) continue;
-                    v[i] = ld_word(left ? from_left + w : from_right + (w - nw));
-                    if (v[i].y != lv || v[i].w != lv) pending |= 1u << i;
-                }
-                // poll the first pending word only, backing off, so that the
-                // polling takes little of the L2 and LSU bandwidth the compute
-                // warps use; once it has arrived, the others have as a rule
-                unsigned nap = 128;
-                for (uint32_t spin = 0; pending && spin < tma::kSpinLimit; ++spin) {
-                    __nanosleep(nap);
-                    nap = nap < 512 ? 2 * nap : 512;
-                    const int first = __ffs(pending) - 1;
-#pragma unroll
-                    for (int i = 0; i < kXB; ++i) {
-                        if (i < first || !((pending >> i) & 1u)) continue;
-                        const int w = base + i * kRX;
-                        v[i] = ld_word(w < nw ? from_left + w : from_right + (w - nw));
-                        if (v[i].y == lv && v[i].w == lv) pending &= ~(1u << i);
-                        else break;
+            for (int i = 0; i < kMaxXW; ++i) {
+                const int w = tid + i * kRT;
+                if (xdst[i] < 0) continue;
+                ulonglong2 v = stage[w];
+                if (!word_is(v, tag)) {
+                    const ulonglong2* g = w < nw ? from_left + w : from_right + (w - nw);
+                    uint32_t spin = 0;
+                    for (; spin < tma::kSpinLimit; ++spin) {
+                        v = ld_word(g);
+                        if (word_is(v, tag)) break;
+                        __nanosleep(64);
                     }
+                    ok = ok && spin < tma::kSpinLimit;
                 }
-                ok = pending == 0;
-#pragma unroll
-                for (int i = 0; i < kXB; ++i) {
-                    const int w = base + i * kRX;
-                    const bool left = w < nw;
-                    if (!ok || w >= 2 * nw || (left ? sl.left : sl.right) < 0) continue;
-                    const int vv = 2 * (left ? w : w - nw), c = vv / a.ldz, z = vv - (vv / a.ldz) * a.ldz;
-                    const int col = left ? c - 4 : sl.w + c;
-                    *reinterpret_cast<float2*>(A + (col + 4) * lds + 4 + z) =
-                        make_float2(__uint_as_float(v[i].x), __uint_as_float(v[i].z));
-                }
+                *reinterpret_cast<float2*>(B + xdst[i]) =
+                    make_float2(__uint_as_float((unsigned)v.x), __uint_as_float((unsigned)v.y));
             }
             if (!ok) {
                 atomicExch(a.err, 1);
                 abort_flag = 1;
             }
-            bar_arrive(1, kRT);
         }
         __syncthreads();
         done = abort_flag != 0;
@@ -505,11 +580,14 @@ int fwd_res_max_rec() { return kRecPerThread * kRC; }
 int fwd_res_max_src() { return kMaxSrc; }
 bool fwd_res_fits(int w, int ldz) {
     const Sched sc = make_sched(w, ldz);
-    return sc.pint + sc.pedge <= kMaxPasses;
+    return sc.pint + sc.pedge <= kMaxPasses && 4 * ldz <= kMaxXW * kRT;
 }
 
+size_t fwd_res_stage_smem(int ldz) { return (size_t)4 * ldz * sizeof(ulonglong2); }
+
 size_t fwd_res_smem(int wmax, int ldz) {
-    const size_t need = (size_t)2 * (wmax + 8) * (ldz + 8) * sizeof(float);
+    // two field buffers of (wmax + 8) columns, then the staging of 4 ldz halo words
+    const size_t need = (size_t)2 * (wmax + 8) * (ldz + 8) * sizeof(float) + fwd_res_stage_smem(ldz);
     return need < kMinSmem ? kMinSmem : need;
 }
 

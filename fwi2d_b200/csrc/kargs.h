@@ -119,8 +119,8 @@ struct FwdResArgs {
     const float* in_old;      // Q^{t-1} at t_begin
     float* out_cur;           // Q^t at t_end
     float* out_old;           // Q^{t-1} at t_end
-    uint4* xbuf;              // halo words {v0, level, v1, level}: [2 parities][nslab][2 sides][2 ldz],
-                              // zero at launch
+    ulonglong2* xbuf;         // halo words, two (value | level << 32) halves each:
+                              // [2 parities][nslab][2 sides][2 ldz], zero at launch
     int* err;
 };
 

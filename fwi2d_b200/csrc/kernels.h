@@ -45,8 +45,9 @@ cudaError_t launch_fwd_loop(int TX, int S, int B, const FwdLoopMaps& maps, const
 int fwd_res_threads();               // compute threads per CTA
 int fwd_res_max_rec();               // receiver entries per slab
 int fwd_res_max_src();               // injection points per slab
-bool fwd_res_fits(int w, int ldz);   // a slab of w columns fits the kernel's TMEM item table
+bool fwd_res_fits(int w, int ldz);   // a slab of w columns fits the kernel's item and halo tables
 size_t fwd_res_smem(int wmax, int ldz);  // dynamic shared memory for slabs up to wmax columns
+size_t fwd_res_stage_smem(int ldz);      // of which the halo staging
 size_t fwd_res_static_smem();
 cudaError_t fwd_res_configure(size_t smem, int* ctas_per_sm);
 cudaError_t launch_fwd_res(const FwdResArgs& a, size_t smem, cudaStream_t st);

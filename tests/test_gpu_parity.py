@@ -123,6 +123,19 @@ def test_forward_variants_agree_on_wide_grid(tmp_path):
         assert rel_l2(o, base) < 1e-5, v
 
 
+def test_resident_kernel_on_benchmark_survey(tmp_path):
+    """The benchmark survey's geometry (11 shots of 351 x 701 with the ABC):
+    the resident kernel splits every shot over 13 CTAs that exchange halos
+    every level; it must agree with the streaming multi-level kernel."""
+    outs = {}
+    for v in ("loop:16,3", "resident"):
+        c, _ = synth.config0(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=400, fwd_kernel=v)
+        with api.Context(c.params, api.MODE_MODELING) as ctx:
+            outs[v] = ctx.model_survey()
+            assert ctx.describe().startswith(v.split(":")[0]), ctx.describe()
+    assert rel_l2(outs["resident"], outs["loop:16,3"]) < 1e-5
+
+
 # ---------------------------------------------------------------------------- random boundary
 def test_random_boundary_bit_exact(case):
     c, vp = case
