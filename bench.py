@@ -58,14 +58,13 @@ def peaks():
 
 def traffic_from_profiles(plan: str):
     """DRAM bytes per launch of the forward kernel variant `plan` uses, from the
-    committed ncu summary (lines 'dram_bytes_per_launch[<variant>]: <bytes>',
-    <variant> as the plan string starts, e.g. 'loop TX=16 S=3')."""
-    f = ROOT / "profiles" / "fwd_loop_kernel_modeling_survey.md"
-    if not f.exists():
-        return None
-    for m in re.finditer(r"dram_bytes_per_launch\[([^\]]+)\]:\s*([0-9.eE+]+)", f.read_text()):
-        if plan.startswith(m.group(1)):
-            return float(m.group(2))
+    committed ncu summaries of the benchmark survey (lines
+    'dram_bytes_per_launch[<variant>]: <bytes>', <variant> as the plan string
+    starts, e.g. 'loop TX=16 S=3' or 'resident')."""
+    for f in sorted((ROOT / "profiles").glob("fwd_*_modeling_survey.md")):
+        for m in re.finditer(r"dram_bytes_per_launch\[([^\]]+)\]:\s*([0-9.eE+]+)", f.read_text()):
+            if plan.startswith(m.group(1)):
+                return float(m.group(2))
     return None
 
 
