@@ -25,10 +25,10 @@
 //     wrote it (the low-latency protocol of NCCL's LL transport), so the
 //     reader checks the data itself: no fence and no flag.  A level computes
 //     the slab's two edge runs first and their threads publish the results
-//     at once; then the interior, during whose last pass every thread starts
-//     asynchronous copies (cp.async, L2 -> shared memory) of its share of the
-//     neighbours' edges, published a whole interior earlier; after the pass
-//     it checks the levels and unpacks them into the halo.  The copies never
+//     at once; then the interior, during whose last two passes every thread
+//     starts asynchronous copies (cp.async, L2 -> shared memory) of its share
+//     of the neighbours' edges, published most of a level earlier; after the
+//     last pass it checks the levels and unpacks them into the halo.  The copies never
 //     stall the compute warps (loads issued to L2 by warps of their own,
 //     queued behind the compute warps' shared-memory traffic, took longer
 //     than the whole interior), and the only barrier is the one per level.
@@ -97,10 +97,10 @@ __device__ __forceinline__ int entry_column(const int* colptr, int col_off, int 
 // Work of a slab per level, in 4 x 4 items (4 rows of a 4-column run): the
 // two edge runs 0 and nruns-1 first — they read the halo and the neighbours
 // wait for their results — then the interior runs 1..nruns-2, which read only
-// the slab's own columns.  Pass k of a thread holds edge item tid + k*kRC
-// (k < pedge) or interior item tid + (k-pedge)*kRC.
+// the slab's own columns, in one stream: pass k of a thread holds item
+// tid + k*kRC, so no pass is left part-empty by the edges.
 struct Sched {
-    int qg, nruns, nint, nedge, pint, pedge;
+    int qg, nruns, nint, nedge, passes;
 };
 __host__ __device__ __forceinline__ Sched make_sched(int w, int ldz) {
     Sched sc;
@@ -108,26 +108,24 @@ __host__ __device__ __forceinline__ Sched make_sched(int w, int ldz) {
     sc.nruns = (w + 3) / 4;
     sc.nedge = (sc.nruns < 2 ? sc.nruns : 2) * sc.qg;
     sc.nint = sc.nruns * sc.qg - sc.nedge;
-    sc.pint = (sc.nint + kRC - 1) / kRC;
-    sc.pedge = (sc.nedge + kRC - 1) / kRC;
+    sc.passes = (sc.nedge + sc.nint + kRC - 1) / kRC;
     return sc;
 }
 // Position (c0, gz) of pass k's item; false when the thread has none in that
 // pass (the position is then run 0's, a safe place to read).
 __device__ __forceinline__ bool item_of(const Sched& sc, int tid, int k, int* c0, int* gz) {
-    int i, run;
-    bool valid;
-    if (k < sc.pedge) {
-        i = tid + k * kRC;
-        valid = i < sc.nedge;
-        run = (valid && i >= sc.qg) ? sc.nruns - 1 : 0;
-    } else {
-        i = tid + (k - sc.pedge) * kRC;
-        valid = i < sc.nint;
-        run = valid ? 1 + i / sc.qg : 0;
+    const int i = tid + k * kRC;
+    int run = 0, q = 0;
+    const bool valid = i < sc.nedge + sc.nint;
+    if (valid && i < sc.nedge) {
+        run = i >= sc.qg ? sc.nruns - 1 : 0;
+        q = i % sc.qg;
+    } else if (valid) {
+        run = 1 + (i - sc.nedge) / sc.qg;
+        q = (i - sc.nedge) % sc.qg;
     }
     *c0 = 4 * run;
-    *gz = valid ? 4 * (i % sc.qg) : 0;
+    *gz = 4 * q;
     return valid;
 }
 
@@ -331,7 +329,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     const int lds = a.ldz + 8;  // stored column: 4 zero rows, ldz rows, 4 zero rows
     const int qg = a.ldz / 4;   // 4-row groups per column
     const Sched sc = make_sched(sl.w, a.ldz);
-    const int passes = sc.pint + sc.pedge;
+    const int passes = sc.passes;
     const long long so = (long long)sl.s * a.fstride;
     // the two field buffers, as offsets into smem (the Q^t / Q^{t-1} roles
     // swap every level; offsets keep every access a shared-memory one)
@@ -460,8 +458,8 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     __syncthreads();
 
     ulonglong2* stage = reinterpret_cast<ulonglong2*>(smem + 2 * (size_t)(a.wmax + 8) * lds);
-    // the halo of the next level is fetched during the last pass
-    const int fetch_at = passes - 1 > sc.pedge ? passes - 1 : sc.pedge;
+    // the halo of the next level is fetched during the last two passes
+    const int fetch_at = passes >= 2 ? passes - 2 : 0;
     bool done = !fits;
     for (int t = a.t_begin; t < a.t_end && !done; ++t) {
         float* A = smem + oa;  // Q^t (stencil)
@@ -493,8 +491,8 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
             const int pos = s_pos[k * kRC + tid];
             const bool valid = pos >= 0;
             const int c0 = (pos >> 16) & 0x3fff, gz = pos & 0xffff;
-            ulonglong2* pa = (k < sc.pedge && sl.left >= 0 && c0 == 0) ? mine : nullptr;
-            ulonglong2* pb = (k < sc.pedge && sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
+            ulonglong2* pa = (sl.left >= 0 && c0 == 0) ? mine : nullptr;  // the edge runs
+            ulonglong2* pb = (sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
             res_item(a, A, B, lds, c0, gz, valid, (pos & 0x40000000) != 0, tbase + kItemCols * k, src, sample, pa, pb,
                      tag);
         }
@@ -580,7 +578,7 @@ int fwd_res_max_rec() { return kRecPerThread * kRC; }
 int fwd_res_max_src() { return kMaxSrc; }
 bool fwd_res_fits(int w, int ldz) {
     const Sched sc = make_sched(w, ldz);
-    return sc.pint + sc.pedge <= kMaxPasses && 4 * ldz <= kMaxXW * kRT;
+    return sc.passes <= kMaxPasses && 4 * ldz <= kMaxXW * kRT;
 }
 
 size_t fwd_res_stage_smem(int ldz) { return (size_t)4 * ldz * sizeof(ulonglong2); }
