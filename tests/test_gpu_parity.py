@@ -136,6 +136,37 @@ def test_resident_kernel_on_benchmark_survey(tmp_path):
     assert rel_l2(outs["resident"], outs["loop:16,3"]) < 1e-5
 
 
+def test_resident_kernel_migration_on_benchmark_geometry(tmp_path):
+    """RTM of the benchmark geometry: the forward through the random boundary
+    runs with a velocity per shot; the resident and the streaming forward
+    kernels (same backward kernel) must give the same image."""
+    imgs = {}
+    data = None
+    for v in ("loop:16,3", "resident"):
+        c, vp = synth.config0(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=300, fwd_kernel=v,
+                              bwd_kernel="loop:16,3")
+        if data is None:
+            with api.Context(c.params, api.MODE_MODELING) as ctx:
+                data = ctx.model_survey()
+        with api.Context(c.params, api.MODE_MIGRATION) as ctx:
+            ctx.set_model(synth.smooth_model(vp, c.dh, 150.0))
+            ctx.rtm_reset()
+            ctx.rtm_survey(data)
+            imgs[v] = ctx.rtm_raw()[0]
+            assert ctx.describe().startswith(v.split(":")[0]), ctx.describe()
+    assert rel_l2(imgs["resident"], imgs["loop:16,3"]) < 1e-5
+
+
+def test_resident_kernel_refuses_a_survey_that_does_not_fit(tmp_path):
+    """A column of more than 384 padded rows does not fit the resident kernel's
+    tables: asked for it explicitly, the context fails with FWI_ERR_PARAM."""
+    c, _ = synth.small_case(tmp_path, nz=380, nx=64, nt=50, nshots=1, nrec=8, fwd_kernel="resident")
+    with api.Context(c.params, api.MODE_MODELING) as ctx:
+        with pytest.raises(api.FwiError) as e:
+            ctx.model_survey()
+    assert e.value.code == -1
+
+
 # ---------------------------------------------------------------------------- random boundary
 def test_random_boundary_bit_exact(case):
     c, vp = case
