@@ -37,7 +37,9 @@ void Engine::sync(const char* what) {
         check(cudaMemcpy(&err, d_err_, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
         if (err) {
             cudaMemset(d_err_, 0, sizeof(int));
-            throw Error(FWI_ERR_TIMEOUT, std::string(what) + ": a kernel's bounded wait for its tile loads gave up");
+            throw Error(FWI_ERR_TIMEOUT, std::string(what) +
+                                             ": a kernel gave up a bounded wait (tile loads, halo exchange) or met a "
+                                             "slab its tables do not hold");
         }
     }
 }
