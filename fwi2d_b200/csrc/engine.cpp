@@ -852,7 +852,7 @@ bool Engine::plan_resident(const Grid& g, const Tables& t, int ns, FwdPlan* p) {
     const size_t smem = fwd_res_smem((wmax + 3) / 4 * 4, g.ldz);
     if (!fwd_res_fits(wmax, g.ldz) || smem > max_dyn) return false;
     int ctas = 0;
-    if (fwd_res_configure(smem, &ctas) != cudaSuccess || ctas < 1) {
+    if (fwd_res_configure(g.ldz, smem, &ctas) != cudaSuccess || ctas < 1) {
         cudaGetLastError();
         return false;
     }

@@ -317,6 +317,9 @@ __device__ __forceinline__ void res_item(const FwdResArgs& a, const float* A, fl
     }
 }
 
+// LDS: the stored column pitch ldz + 8 when known at compile time (every
+// shared-memory offset of the stencil becomes an immediate), 0 for any ldz.
+template <int LDS>
 __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ SrcList src;
@@ -326,7 +329,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     const int tid = threadIdx.x, warp = tid >> 5;
     const ResSlab sl = a.slabs[blockIdx.x];
     const ShotDesc sd = a.shots[sl.s];
-    const int lds = a.ldz + 8;  // stored column: 4 zero rows, ldz rows, 4 zero rows
+    const int lds = LDS ? LDS : a.ldz + 8;  // stored column: 4 zero rows, ldz rows, 4 zero rows
     const int qg = a.ldz / 4;   // 4-row groups per column
     const Sched sc = make_sched(sl.w, a.ldz);
     const int passes = sc.passes;
@@ -558,17 +561,28 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
 // can take all 512 TMEM columns.
 constexpr size_t kMinSmem = 116 * 1024;
 
-cudaError_t res_configure(size_t smem, int* ctas) {
+// column pitches (ldz + 8) compiled as constants: ldz a multiple of 32 up to 384
+#define FWI_FWD_RES_LDS(X) X(40) X(72) X(104) X(136) X(168) X(200) X(232) X(264) X(296) X(328) X(360) X(392)
+
+const void* res_kernel(int ldz) {
+#define FWI_X(l) if (ldz + 8 == l) return (const void*)fwd_res_kernel<l>;
+    FWI_FWD_RES_LDS(FWI_X)
+#undef FWI_X
+    return (const void*)fwd_res_kernel<0>;
+}
+
+cudaError_t res_configure(int ldz, size_t smem, int* ctas) {
     smem = smem < kMinSmem ? kMinSmem : smem;
-    cudaError_t e = cudaFuncSetAttribute(fwd_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fwd_res_kernel, kRT, smem);
+    const void* fn = res_kernel(ldz);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, kRT, smem);
     return e;
 }
 
 cudaError_t res_launch(const FwdResArgs& a, size_t smem, cudaStream_t st) {
     smem = smem < kMinSmem ? kMinSmem : smem;
     void* args[] = {const_cast<FwdResArgs*>(&a)};
-    return cudaLaunchCooperativeKernel((const void*)fwd_res_kernel, dim3(a.nslab), dim3(kRT), args, smem, st);
+    return cudaLaunchCooperativeKernel(res_kernel(a.ldz), dim3(a.nslab), dim3(kRT), args, smem, st);
 }
 
 }  // namespace
@@ -591,14 +605,14 @@ size_t fwd_res_smem(int wmax, int ldz) {
 
 size_t fwd_res_static_smem() {
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, fwd_res_kernel) != cudaSuccess) {
+    if (cudaFuncGetAttributes(&fa, fwd_res_kernel<0>) != cudaSuccess) {
         cudaGetLastError();
         return sizeof(SrcList) + 64;
     }
     return fa.sharedSizeBytes;
 }
 
-cudaError_t fwd_res_configure(size_t smem, int* ctas_per_sm) { return res_configure(smem, ctas_per_sm); }
+cudaError_t fwd_res_configure(int ldz, size_t smem, int* ctas_per_sm) { return res_configure(ldz, smem, ctas_per_sm); }
 
 cudaError_t launch_fwd_res(const FwdResArgs& a, size_t smem, cudaStream_t st) { return res_launch(a, smem, st); }
 

@@ -49,7 +49,7 @@ bool fwd_res_fits(int w, int ldz);   // a slab of w columns fits the kernel's it
 size_t fwd_res_smem(int wmax, int ldz);  // dynamic shared memory for slabs up to wmax columns
 size_t fwd_res_stage_smem(int ldz);      // of which the halo staging
 size_t fwd_res_static_smem();
-cudaError_t fwd_res_configure(size_t smem, int* ctas_per_sm);
+cudaError_t fwd_res_configure(int ldz, size_t smem, int* ctas_per_sm);
 cudaError_t launch_fwd_res(const FwdResArgs& a, size_t smem, cudaStream_t st);
 
 // ---- k_bwd_loop.cu -------------------------------------------------------------
