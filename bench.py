@@ -126,7 +126,7 @@ def dist_env():
 def make_case():
     from fwi2d_b200 import synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_bench_"))
-    case, vp = synth.config0(d, seed=0)
+    case, vp = synth.modeling_survey(d, seed=0)
     return case, vp
 
 
@@ -223,7 +223,7 @@ def profile_case(which: str = "large"):
     if which == "batched":
         # 60 of the 240 windowed shots (every 4th), nt 40: one RTM = one
         # forward and one backward multi-level launch, fields ~1.9 GB > L2
-        case, _ = synth.config3(d, every=4, nt=40)
+        case, _ = synth.aperture_survey(d, every=4, nt=40)
         with api.Context(case.params, api.MODE_MIGRATION) as ctx:
             dims = ctx.dims
             ctx.rtm_reset()
@@ -231,12 +231,12 @@ def profile_case(which: str = "large"):
             print("profile case done:", ctx.describe())
         return
     if which == "small":
-        case, _ = synth.config0(d, seed=0)
+        case, _ = synth.modeling_survey(d, seed=0)
     elif which == "resident":
         # the benchmark survey with the shared-memory-resident kernel, nt 200
-        case, _ = synth.config0(d, seed=0, nt=200, fwd_kernel="resident")
+        case, _ = synth.modeling_survey(d, seed=0, nt=200, fwd_kernel="resident")
     else:
-        case, _ = synth.config2(d, seed=2, nt=40)
+        case, _ = synth.fwi_survey(d, seed=2, nt=40)
     with api.Context(case.params, api.MODE_MODELING) as ctx:
         ctx.model_survey_raw()
         print("profile case done:", ctx.describe())
@@ -249,7 +249,7 @@ def batched_survey(peak: float, nt: int = 300, reps: int = 2) -> dict:
     backward kernels timed by CUDA events on the engine stream."""
     from fwi2d_b200 import api, synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_batched_"))
-    case, _ = synth.config3(d, nt=nt)
+    case, _ = synth.aperture_survey(d, nt=nt)
     with api.Context(case.params, api.MODE_MIGRATION) as ctx:
         dims = ctx.dims
         widths = [ctx.window(s)[1] for s in range(dims.nsrc)]
@@ -387,7 +387,7 @@ def main():
     line = {
         "metric": "FD grid-pt updates/s", "value": value, "unit": "grid-pt updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 4-layer + anomaly model, config 0)",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 4-layer + anomaly model, 151x501 at 10 m)",
         "config": {"workload": WORKLOAD, "shots_per_rank": d.nsrc, "grid": [d.nzz, d.nxx], "time_steps": n_steps,
                    "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"shot replicas x{world}"},
         "e2e": {"value": world * ups / (e2e_ms * 1e-3), "unit": "grid-pt updates/s", "ms_per_step": e2e_ms,

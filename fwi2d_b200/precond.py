@@ -259,7 +259,7 @@ def time_to_error(log: FwiLog, target: float) -> float | None:
 def main(argv=None) -> int:
     """Train the preconditioner and compare CNN-preconditioned with plain FWI.
 
-    python -m fwi2d_b200.precond --models 128 --stages 4 --epochs 40 --iterations 10 --test small|config3
+    python -m fwi2d_b200.precond --models 128 --stages 4 --epochs 40 --iterations 10 --test small|aperture
     writes a JSON summary (--out) with the training history and both runs'
     misfit, model-error and wall-time trajectories."""
     import argparse
@@ -273,8 +273,8 @@ def main(argv=None) -> int:
     ap.add_argument("--stages", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--iterations", type=int, default=10)
-    ap.add_argument("--test", choices=["small", "config3"], default="small")
-    ap.add_argument("--nt", type=int, default=None, help="time samples of the config3 test (default 4001)")
+    ap.add_argument("--test", choices=["small", "aperture"], default="small")
+    ap.add_argument("--nt", type=int, default=None, help="time samples of the aperture-survey test (default 4001)")
     ap.add_argument("--target", type=float, default=0.03)
     ap.add_argument("--out", default=None)
     ap.add_argument("--weights", default=None, help="save / load the trained network here")
@@ -302,7 +302,7 @@ def main(argv=None) -> int:
         vs = start_model(vt, s.dh)
     else:
         kw = {"nt": a.nt} if a.nt else {}
-        case, vt = synth.config3(root / "test", **kw)
+        case, vt = synth.aperture_survey(root / "test", **kw)
         vs = synth.gradient_model(vt, case.dh)
     runs = {}
     for mode in ("plain", "cnn"):

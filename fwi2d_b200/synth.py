@@ -148,7 +148,7 @@ def write_case(root: str | os.PathLike, vp: np.ndarray, dh: float, nt: int, dt: 
 
 
 # ---------------------------------------------------------------- workloads
-def config0(root, seed: int = 0, **over) -> tuple[Case, np.ndarray]:
+def modeling_survey(root, seed: int = 0, **over) -> tuple[Case, np.ndarray]:
     """Plain forward modeling: 151 x 501 at 10 m, 11 shots every 500 m,
     251 receivers every 20 m at 10 m depth, 30 Hz, dt 1 ms, nt 3001, 100-cell boundary."""
     nz, nx, dh = 151, 501, 10.0
@@ -162,7 +162,7 @@ def config0(root, seed: int = 0, **over) -> tuple[Case, np.ndarray]:
     return case, vp
 
 
-def config2(root, seed: int = 2, **over) -> tuple[Case, np.ndarray]:
+def fwi_survey(root, seed: int = 2, **over) -> tuple[Case, np.ndarray]:
     """Plain FWI: 301 x 1701 at 10 m, 81 shots every 200 m, 851 receivers every
     20 m, 15 Hz, dt 1 ms, nt 4001, 100-cell boundaries."""
     nz, nx, dh = 301, 1701, 10.0
@@ -177,8 +177,8 @@ def config2(root, seed: int = 2, **over) -> tuple[Case, np.ndarray]:
     return case, vp
 
 
-def config3(root, seed: int = 3, every: int = 1, **over) -> tuple[Case, np.ndarray]:
-    """Batched uneven-aperture FWI: the config-2 model and receiver spread,
+def aperture_survey(root, seed: int = 3, every: int = 1, **over) -> tuple[Case, np.ndarray]:
+    """Batched uneven-aperture FWI: the FWI survey's model and receiver spread,
     240 shots every 70 m, each modeled on the columns within its own maximum
     offset (uniform 1.5-8 km from the seed; windows of about 300-1700 columns).
     every > 1 keeps every every-th shot (smaller profiling cases)."""

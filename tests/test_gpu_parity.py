@@ -129,7 +129,7 @@ def test_resident_kernel_on_benchmark_survey(tmp_path):
     every level; it must agree with the streaming multi-level kernel."""
     outs = {}
     for v in ("loop:16,3", "resident"):
-        c, _ = synth.config0(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=400, fwd_kernel=v)
+        c, _ = synth.modeling_survey(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=400, fwd_kernel=v)
         with api.Context(c.params, api.MODE_MODELING) as ctx:
             outs[v] = ctx.model_survey()
             assert ctx.describe().startswith(v.split(":")[0]), ctx.describe()
@@ -143,7 +143,7 @@ def test_resident_kernel_migration_on_benchmark_geometry(tmp_path):
     imgs = {}
     data = None
     for v in ("loop:16,3", "resident"):
-        c, vp = synth.config0(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=300, fwd_kernel=v,
+        c, vp = synth.modeling_survey(tmp_path / v.replace(":", "_").replace(",", "_"), seed=0, nt=300, fwd_kernel=v,
                               bwd_kernel="loop:16,3")
         if data is None:
             with api.Context(c.params, api.MODE_MODELING) as ctx:
