@@ -60,12 +60,18 @@ def traffic_from_profiles(plan: str):
     """DRAM bytes per launch of the forward kernel variant `plan` uses, from the
     committed ncu summaries of the benchmark survey (lines
     'dram_bytes_per_launch[<variant>]: <bytes>', <variant> as the plan string
-    starts, e.g. 'loop TX=16 S=3' or 'resident')."""
+    starts, e.g. 'loop TX=16 S=3' or 'resident').  Returns (bytes, source):
+    the profile file the figure comes from, or (None, why) when no capture of
+    this variant is committed, so a missing figure is reported as missing."""
     for f in sorted((ROOT / "profiles").glob("fwd_*_modeling_survey.md")):
         for m in re.finditer(r"dram_bytes_per_launch\[([^\]]+)\]:\s*([0-9.eE+]+)", f.read_text()):
             if plan.startswith(m.group(1)):
-                return float(m.group(2))
-    return None
+                return float(m.group(2)), f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of " \
+                                          f"'{m.group(1)}' on this survey, {f.relative_to(ROOT)}"
+    variant = plan.split("|")[0].strip()
+    print(f"bench: no committed ncu capture of the forward variant '{variant}': roofline.traffic is null",
+          file=sys.stderr)
+    return None, f"missing: no ncu capture of '{variant}' in profiles/"
 
 
 class Clocks:
@@ -191,6 +197,10 @@ def run_reference(args, rank, world):
                                             "'Run time' (shot loop incl. per-shot file writes); runs on the B200"},
                     e2e={"value": value, "unit": "grid-pt updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                     reference_build="oracle/_ref/modeling.exe", slowest_step_s=t)
+        if not args.no_batched:
+            back = reference_backward(case, vp)
+            if back:
+                line["backward_loops"] = back
     else:
         cb = cpu_baseline(case, vp)
         line.update(value=cb["value"], ms_per_step=None, cpu_baseline=dict(cb, kind="port"),
@@ -277,6 +287,148 @@ def batched_survey(peak: float, nt: int = 300, reps: int = 2) -> dict:
     }
 
 
+def rtm_benchmark_geometry(reps: int = 2) -> dict:
+    """RTM and FWI-gradient back-propagation on the benchmark survey's geometry
+    (11 shots, 351 x 701 padded, nt 3001 + 119 levels; migration in the
+    Gaussian-smoothed model, as configuration 1), timed per kernel with CUDA
+    events on the engine stream.  The reference arm times its own loops on the
+    same geometry (oracle/_ref/ref_harness --time): forward_solver without ABC
+    (modeling.cu:286-299), inject_seismogram + cross_correlation
+    (migration.cu:61-81) and inject_adjoint + build_gradient
+    (inversion.cu:230-248).  The input traces are seeded noise: the timing does
+    not depend on their values."""
+    from fwi2d_b200 import api, synth
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_rtm_"))
+    case, vp = synth.modeling_survey(d, seed=0)
+    smooth = synth.smooth_model(vp, case.dh, 150.0)
+    out = {"workload": "RTM / FWI gradient of the plain modeling survey's geometry: 11 shots, 351x701 padded "
+                       "(100-cell random boundary), 251 receivers, nt 3001 + 119 levels"}
+    for mode, key in ((api.MODE_MIGRATION, "rtm"), (api.MODE_INVERSION, "gradient")):
+        with api.Context(case.params, mode) as ctx:
+            dims = ctx.dims
+            data = (np.random.default_rng(1).standard_normal(dims.nsrc * dims.nrec * dims.nt) * 1e-3).astype(
+                np.float32)
+            ctx.set_model(smooth)
+            if mode == api.MODE_MIGRATION:
+                run = lambda: (ctx.rtm_reset(), ctx.rtm_survey_raw(data))
+            else:
+                ctx.set_observed_raw(data)
+                run = lambda: ctx.compute_gradient(True)
+            run()  # autotune + warm-up
+            ctx.fwd_timing(True)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                run()
+            wall = (time.perf_counter() - t0) / reps
+            fms, fn, fu = ctx.fwd_timing_read()
+            bms, bn, bu = ctx.bwd_timing_read()
+            ctx.fwd_timing(False)
+            out[key] = {"backward_updates_per_s": bu / (bms * 1e-3), "backward_ms": bms / reps,
+                        "forward_updates_per_s": fu / (fms * 1e-3), "forward_ms": fms / reps,
+                        "survey_wall_s": wall, "plans": ctx.describe()}
+    return out
+
+
+def fwi_measure(case, vp_true: np.ndarray, iterations: int) -> dict:
+    """The reference's FWI iteration (inversion_main.cpp:13-22: compute_gradient,
+    optimization = two line-search modelings + the parabola, update_model;
+    inversion.cu:111-358) from the 1-D depth-gradient model, through the C ABI;
+    observed data modeled in the true model by the same engine.  Reports the
+    wall time per iteration and the misfit and relative model RMS error after
+    each."""
+    import torch
+
+    from fwi2d_b200 import api, synth
+    init = synth.gradient_model(vp_true, case.dh)
+    vt = vp_true.astype(np.float64)
+    err = lambda v: float(np.sqrt(np.mean((v.astype(np.float64) - vt) ** 2)) / np.sqrt(np.mean(vt ** 2)))
+    with api.Context(case.params, api.MODE_INVERSION) as ctx:
+        dims = ctx.dims
+        seis = torch.empty(dims.nsrc * dims.nrec * dims.nt, dtype=torch.float32, device="cuda")
+        ctx.set_model(vp_true)
+        ctx.model_survey_dev(seis.data_ptr())
+        ctx.set_model(init)
+        ctx.set_observed_dev(seis.data_ptr())
+        torch.cuda.synchronize()
+        res = {"shots": dims.nsrc, "grid": [dims.nzz, dims.nxx], "levels": dims.nt + dims.tlag,
+               "iterations": iterations, "misfit": [], "model_error": [err(init)], "step": [], "seconds": []}
+        for _ in range(iterations):
+            t0 = time.perf_counter()
+            sum_res = ctx.compute_gradient(True)
+            f0 = float(np.sqrt(np.float32(sum_res)))
+            step = ctx.optimization(f0)
+            v = ctx.update_model(step)
+            res["seconds"].append(time.perf_counter() - t0)
+            res["misfit"].append(f0)
+            res["step"].append(float(step))
+            res["model_error"].append(err(v))
+        res["s_per_iteration"] = float(np.mean(res["seconds"]))
+        res["shots_per_s"] = dims.nsrc / res["s_per_iteration"]
+        res["plans"] = ctx.describe()
+    return res
+
+
+def fwi_surveys(iters_plain: int = 5, iters_batched: int = 1) -> dict:
+    """Configurations 2 and 3 as FWI: the 81-shot survey on the 301x1701 dipping
+    model (501x1901 padded, nt 4001) and the 240-shot survey of per-shot
+    aperture windows on the same model."""
+    from fwi2d_b200 import synth
+    out = {}
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_fwi_"))
+    for key, make, iters in (("plain_fwi", synth.fwi_survey, iters_plain),
+                             ("batched_fwi", synth.aperture_survey, iters_batched)):
+        if iters <= 0:
+            continue
+        try:
+            case, vp = make(d / key)
+            out[key] = fwi_measure(case, vp, iters)
+        except Exception as e:  # report, never lose the headline line
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+    out["plain_fwi_workload"] = ("81 shots every 200 m, 851 receivers, 301x1701 @10 m dipping model + 100-cell "
+                                 "boundaries, 15 Hz, dt 1 ms, nt 4001, 1-D depth-gradient start")
+    out["batched_fwi_workload"] = ("240 shots every 70 m with aperture windows 300-1700 columns, same model, "
+                                   "receivers and time axis, all shots of a propagation in one launch per batch")
+    return out
+
+
+def reference_backward(case, vp, reps: int = 3) -> dict | None:
+    """The reference's own forward, migration and adjoint loops on the benchmark
+    geometry, run by oracle/_ref/ref_harness --time (built from the reference
+    sources; the boundary velocity is an input because the reference's
+    random-boundary kernels index out of bounds), CUDA events per loop."""
+    from fwi2d_b200 import synth
+    from oracle import oracle as O
+    exe = ROOT / "oracle" / "_ref" / "ref_harness"
+    if not exe.exists():
+        return None
+    nb = 100
+    smooth = synth.smooth_model(vp, case.dh, 150.0)
+    base = O.expand(smooth, nb)
+    bt = O.bumps(base.shape[1], base.shape[0], nb, case.dh, 200.0, 500.0, 0, 0)
+    vel = O.rbc(base, nb, case.dh, 500.0, float(smooth.min()), float(smooth.max()), 0, 0, bt)
+    vfile = case.root / "ref_vel.bin"
+    np.ascontiguousarray(vel.T, dtype=np.float32).tofile(vfile)
+    rng = np.random.default_rng(1)
+    for k in range(len(case.sx)):
+        (rng.standard_normal(case.nt * len(case.rx)) * 1e-3).astype(np.float32).tofile(
+            case.root / f"ref_data_{k + 1}.bin")
+    r = subprocess.run([str(exe), "--time", str(case.params), str(vfile), str(case.root / "ref_data_"), str(reps)],
+                       capture_output=True, text=True, cwd=str(case.root), timeout=900,
+                       env=dict(os.environ, TERM=os.environ.get("TERM", "dumb")))
+    if r.returncode != 0:
+        return {"error": f"ref_harness --time rc={r.returncode}: {r.stderr[-300:]}"}
+    rows = [dict(kv.split("=") for kv in ln.split()[1:]) for ln in r.stdout.splitlines() if ln.startswith("time ")]
+    rows = rows[1:] if len(rows) > 1 else rows  # the first repetition warms up
+    ups = float(rows[0]["updates"])
+    mean = lambda k: float(np.mean([float(x[k]) for x in rows]))
+    return {"workload": "the reference's loops on the plain modeling survey's geometry: 11 shots, 351x701 padded, "
+                        "nt 3001 + 119 levels, boundary velocity given",
+            "forward_rbc": {"updates_per_s": ups / (mean("fwd_ms") * 1e-3), "ms": mean("fwd_ms")},
+            "rtm_backward": {"updates_per_s": ups / (mean("rtm_bwd_ms") * 1e-3), "ms": mean("rtm_bwd_ms")},
+            "gradient_backward": {"updates_per_s": ups / (mean("grad_bwd_ms") * 1e-3), "ms": mean("grad_bwd_ms")},
+            "reference_build": "oracle/_ref/ref_harness", "repetitions_timed": len(rows)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -285,6 +437,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-survey companion measurement")
+    ap.add_argument("--fwi-iterations", type=int, default=5,
+                    help="FWI iterations of the 81-shot survey companion measurement (0: skip)")
+    ap.add_argument("--fwi-batched-iterations", type=int, default=1,
+                    help="FWI iterations of the 240-shot windowed survey companion measurement (0: skip)")
     ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small", "batched", "unet", "resident"],
                     help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
                          "time axis; small: the benchmark survey)")
@@ -383,7 +539,7 @@ def main():
     bytes_per_launch = BYTES_PER_UPDATE * k_updates / k_launches
     avg_launch_ms = k_ms / k_launches
     achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
-    traffic = traffic_from_profiles(plan)
+    traffic, traffic_src = traffic_from_profiles(plan)
     line = {
         "metric": "FD grid-pt updates/s", "value": value, "unit": "grid-pt updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -394,7 +550,8 @@ def main():
                 "h2d_bytes_per_step": int(h_model.numel() * 4), "d2h_bytes_per_step": int(nseis * 4)},
         "roofline": {"bound": "hbm", "kernel": "forward step (" + plan + ")", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
                      "avg_launch_us": 1e3 * avg_launch_ms, "launches_timed": k_launches,
                      "kernel_share_of_step": k_ms / (ms * args.steps),
                      "note": "achieved = 16 B per grid-point update x updates per launch / average launch time "
@@ -412,6 +569,10 @@ def main():
     if world == 1 and not args.no_batched:
         ctx.close()
         line["batched_survey"] = batched_survey(peak)
+        line["rtm_benchmark_geometry"] = rtm_benchmark_geometry()
+    if world == 1 and args.fwi_iterations > 0:
+        ctx.close()
+        line["fwi"] = fwi_surveys(args.fwi_iterations, args.fwi_batched_iterations)
     ctx.close()
     if world > 1:
         torch.distributed.barrier()

@@ -79,6 +79,12 @@ Engine::Engine(const std::string& params_path, int mode) : P_(params_path), mode
     if (const char* e = std::getenv("FWI2D_FWD_KERNEL")) fwd_kernel_ = e;
     bwd_kernel_ = P_.str_or("bwd_kernel", "auto");
     if (const char* e = std::getenv("FWI2D_BWD_KERNEL")) bwd_kernel_ = e;
+    // test hooks of the bounded device waits (tests/test_gpu_failure.py)
+    const uint64_t spin = P_.u64_or("test_wait_limit", 1u << 22);
+    if (spin < 16 || spin > (1u << 22)) throw Error(FWI_ERR_PARAM, "test_wait_limit must lie in [16, 4194304]");
+    spin_limit_ = (unsigned)spin;
+    stall_fwd_ = P_.i_or("test_stall_fwd", -1);
+    stall_bwd_ = P_.i_or("test_stall_bwd", -1);
 
     wavelet_ = make_wavelet(nt_, dt_, fmax_, &tlag_);
     geo_ = read_geometry(P_.str("SPS"), P_.str("RPS"));
@@ -665,6 +671,8 @@ void Engine::launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, cons
     a.out1 = out1;
     a.out2 = out2;
     a.err = d_err_;
+    a.spin = spin_limit_;
+    a.stall = -1;
     const CUtensorMap& mc = tmap(cur, g, batch_, fwd_tma_box_cur_z(c), fwd_tma_box_cur_x(c));
     const CUtensorMap& mo = tmap(old, g, batch_, fwd_tma_box_pt_z(c), fwd_tma_box_pt_x(c));
     const CUtensorMap& mv =
@@ -769,6 +777,8 @@ void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Table
     a.rec_sample0 = a.rec_sample1 = -1;
     a.out1 = a.out2 = nullptr;
     a.err = d_err_;
+    a.spin = spin_limit_;
+    a.stall = stall_fwd_;
     la.t_begin = t_begin;
     la.t_end = t_end;
     la.nt = nt_;
@@ -910,6 +920,8 @@ void Engine::launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables
     a.out_old = out_old;
     a.xbuf = d_xbuf_;
     a.err = d_err_;
+    a.spin = spin_limit_;
+    a.stall = stall_fwd_;
     check(cudaMemsetAsync(d_xbuf_, 0, xb * sizeof(ulonglong2), st_), "memset halo exchange buffer");
     TimedRegion r;
     if (timed_updates >= 0) timing_begin(&r);
@@ -1321,6 +1333,8 @@ void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Table
     a.acc_b = acc_[1];
     a.err = d_err_;
     a.sync = d_sync_;
+    a.spin = spin_limit_;
+    a.stall = stall_bwd_;
     check(cudaMemsetAsync(d_sync_, 0, sizeof(unsigned), st_), "memset grid barrier");
     TimedRegion r;
     if (timed_updates >= 0) timing_begin(&r);

@@ -289,6 +289,13 @@ private:
     ulonglong2* d_xbuf_ = nullptr;
     size_t slabs_cap_ = 0, xbuf_cap_ = 0;
     int sm_count_ = 0;
+    // bounded device waits: polls before a wait gives up (key test_wait_limit,
+    // default 2^22); failure drill (keys test_stall_fwd / test_stall_bwd): the
+    // CTA of that index in the multi-level / resident forward or the
+    // multi-level backward kernel withholds its work so the others' waits run
+    // out (-1: off)
+    unsigned spin_limit_ = 1u << 22;
+    int stall_fwd_ = -1, stall_bwd_ = -1;
     std::string fwd_kernel_ = "auto";  // key fwd_kernel: auto | simple | tma:T,TX,S
     float* fwd_cur_ = nullptr;         // Q^N after run_forward
     float* fwd_old_ = nullptr;         // Q^{N-1}

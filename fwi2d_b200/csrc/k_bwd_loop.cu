@@ -20,8 +20,11 @@
 //     TX/8 columns, register-window Laplacians) and store the four outputs
 //     with coalesced float4 stores, then release the stage.
 //
-// Every wait is bounded (tma::kSpinLimit polls); a wait that gives up raises
-// *err and the kernel returns once its own copies in flight have landed.
+// Every wait is bounded (a.spin polls; a grid-barrier poll also gives up as
+// soon as another CTA has raised *err); a wait that gives up raises *err and
+// the kernel returns once its own copies in flight have landed.  The failure
+// drill (a.stall) makes one CTA withhold the loads of its first tile, so its
+// consumers' and then every other CTA's waits run out.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -55,13 +58,16 @@ struct BMeta {
     int s, x0, z0, nxx, col_off, has_rec;
 };
 
-__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target) {
+// Gives up after `limit` polls, or at once when another CTA has raised *err
+// (that CTA has left the level loop and will never arrive).
+__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, uint32_t limit, const int* err) {
     __threadfence();
     atomicAdd(counter, 1u);
-    for (uint32_t i = 0; i < tma::kSpinLimit; ++i) {
+    for (uint32_t i = 0; i < limit; ++i) {
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
         if (v >= target) return true;
+        if (tma::ld_flag(err)) return false;
         __nanosleep(64);
     }
     return false;
@@ -174,10 +180,11 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                 int kk = k;
                 for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                     const int stg = kk % S;
-                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1))) {
+                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), a.spin)) {
                         ok = false;
                         break;
                     }
+                    if (a.stall == (int)blockIdx.x && b == a.b_begin && kk == k) continue;  // failure drill
                     const ft::TileInfo ti = decode_tile(a, tile, TX);
                     const int s = ti.s, z0 = ti.z0, x0 = ti.x0;
                     const ShotDesc sd = a.shots[s];
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
             int kk = k;
             for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                 const int stg = kk % S;
-                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1))) {
+                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1), a.spin)) {
                     if (lane == 0) atomicExch(a.err, 1);
                     abort_flag = 1;
                     ok = false;
@@ -231,7 +238,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
         // the CTA's tiles of level b are written: grid barrier
         __syncthreads();
         if (tid == 0 && !abort_flag) {
-            if (!grid_barrier(a.sync, (unsigned)(b - a.b_begin + 1) * gridDim.x)) {
+            if (!grid_barrier(a.sync, (unsigned)(b - a.b_begin + 1) * gridDim.x, a.spin, a.err)) {
                 atomicExch(a.err, 1);
                 abort_flag = 1;
             }
@@ -241,7 +248,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
             // never leave copies in flight behind an exiting CTA
             if (tid == kNC)
                 for (int q = (issued > S ? issued - S : 0); q < issued; ++q)
-                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
+                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), a.spin);
             return;
         }
         for (int tile = blockIdx.x; tile < total; tile += gridDim.x) ++k;

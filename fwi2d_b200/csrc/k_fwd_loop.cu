@@ -14,7 +14,10 @@
 // fences, increments a global counter and polls it (bounded, with a short
 // sleep) until every CTA has arrived; the producer then issues a proxy fence so
 // its next TMA reads see the other CTAs' stores.  A poll that gives up raises
-// *err and the kernel returns with no copy in flight.
+// *err and the kernel returns with no copy in flight.  Waits give up after
+// la.base.spin polls; the failure drill (la.base.stall) makes one CTA withhold
+// the loads of its first tile, so its consumers' and then every other CTA's
+// waits run out.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -30,13 +33,16 @@ namespace {
 
 using namespace ft;
 
-__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target) {
+// Gives up after `limit` polls, or at once when another CTA has raised *err
+// (that CTA has left the level loop and will never arrive).
+__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, uint32_t limit, const int* err) {
     __threadfence();
     atomicAdd(counter, 1u);
-    for (uint32_t i = 0; i < tma::kSpinLimit; ++i) {
+    for (uint32_t i = 0; i < limit; ++i) {
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
         if (v >= target) return true;
+        if (tma::ld_flag(err)) return false;
         __nanosleep(64);
     }
     return false;
@@ -91,10 +97,11 @@ __global__ void __launch_bounds__(kNT, MINB)
                 int kk = k;
                 for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                     const int stg = kk % S;
-                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1))) {
+                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), b.spin)) {
                         ok = false;
                         break;
                     }
+                    if (b.stall == (int)blockIdx.x && t == la.t_begin && kk == k) continue;  // failure drill
                     const TileInfo ti = decode(a, tile, TX);
                     const ShotDesc sd = a.shots[ti.s];
                     TileMeta& mt = meta[stg];
@@ -129,7 +136,7 @@ __global__ void __launch_bounds__(kNT, MINB)
             int kk = k;
             for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                 const int stg = kk % S;
-                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1))) {
+                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1), b.spin)) {
                     if (lane == 0) atomicExch(a.err, 1);
                     abort_flag = 1;
                     ok = false;
@@ -178,7 +185,7 @@ __global__ void __launch_bounds__(kNT, MINB)
         // the CTA's tiles of level t are written: grid barrier
         __syncthreads();
         if (tid == 0 && !abort_flag) {
-            if (!grid_barrier(la.sync, (unsigned)(t - la.t_begin + 1) * gridDim.x)) {
+            if (!grid_barrier(la.sync, (unsigned)(t - la.t_begin + 1) * gridDim.x, b.spin, b.err)) {
                 atomicExch(b.err, 1);
                 abort_flag = 1;
             }
@@ -189,7 +196,7 @@ __global__ void __launch_bounds__(kNT, MINB)
             // for the last S loads issued; phases already consumed pass at once
             if (tid == kNC)
                 for (int q = (issued > S ? issued - S : 0); q < issued; ++q)
-                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
+                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), b.spin);
             return;
         }
         // this CTA's tile count per level is fixed: advance the pipeline counter

@@ -37,9 +37,12 @@
 // parity slot two levels later, after it has read its neighbours' next
 // level, which they published only after reading that slot.  It is zeroed
 // before every launch (level 0 is no level).  Every wait is bounded
-// (tma::kSpinLimit polls); a wait that gives up raises *err and the CTA
-// leaves the level loop (with no asynchronous copy in flight and its TMEM
-// released), after which its neighbours' waits run out the same way.
+// (a.spin polls); a wait that gives up raises *err and the CTA leaves the
+// level loop (with no asynchronous copy in flight and its TMEM released).  A
+// poll also gives up as soon as *err is raised, so one failure ends every
+// slab's level loop at its next missing halo word instead of slab after slab
+// through each one's own timeout.  The failure drill (a.stall) makes one slab
+// publish no halo words, so its neighbours' polls run out.
 #include <cuda_runtime.h>
 
 #include "kargs.h"
@@ -463,6 +466,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     ulonglong2* stage = reinterpret_cast<ulonglong2*>(smem + 2 * (size_t)(a.wmax + 8) * lds);
     // the halo of the next level is fetched during the last two passes
     const int fetch_at = passes >= 2 ? passes - 2 : 0;
+    const bool publish = (int)blockIdx.x != a.stall;
     bool done = !fits;
     for (int t = a.t_begin; t < a.t_end && !done; ++t) {
         float* A = smem + oa;  // Q^t (stencil)
@@ -494,8 +498,8 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
             const int pos = s_pos[k * kRC + tid];
             const bool valid = pos >= 0;
             const int c0 = (pos >> 16) & 0x3fff, gz = pos & 0xffff;
-            ulonglong2* pa = (sl.left >= 0 && c0 == 0) ? mine : nullptr;  // the edge runs
-            ulonglong2* pb = (sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
+            ulonglong2* pa = (publish && sl.left >= 0 && c0 == 0) ? mine : nullptr;  // the edge runs
+            ulonglong2* pb = (publish && sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
             res_item(a, A, B, lds, c0, gz, valid, (pos & 0x40000000) != 0, tbase + kItemCols * k, src, sample, pa, pb,
                      tag);
         }
@@ -509,15 +513,19 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
                 const int w = tid + i * kRT;
                 if (xdst[i] < 0) continue;
                 ulonglong2 v = stage[w];
-                if (!word_is(v, tag)) {
+                if (ok && !word_is(v, tag)) {
+                    // after one failure the rest of the halo is not awaited
                     const ulonglong2* g = w < nw ? from_left + w : from_right + (w - nw);
-                    uint32_t spin = 0;
-                    for (; spin < tma::kSpinLimit; ++spin) {
+                    ok = false;
+                    for (uint32_t spin = 0; spin < a.spin; ++spin) {
                         v = ld_word(g);
-                        if (word_is(v, tag)) break;
+                        if (word_is(v, tag)) {
+                            ok = true;
+                            break;
+                        }
+                        if (tma::ld_flag(a.err)) break;
                         __nanosleep(64);
                     }
-                    ok = ok && spin < tma::kSpinLimit;
                 }
                 *reinterpret_cast<float2*>(B + xdst[i]) =
                     make_float2(__uint_as_float((unsigned)v.x), __uint_as_float((unsigned)v.y));

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kNT, 2)
         int k = 0;
         for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
             const int stg = k % S;
-            if (k >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((k / S) - 1) & 1))) {
+            if (k >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((k / S) - 1) & 1), a.spin)) {
                 atomicExch(a.err, 1);
                 break;
             }
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kNT, 2)
         }
         // never leave copies in flight behind an exiting CTA: wait (bounded)
         // for the last S loads issued
-        for (int kk = (k > S ? k - S : 0); kk < k; ++kk) tma::mbar_wait(&full[kk % S], (uint32_t)((kk / S) & 1));
+        for (int kk = (k > S ? k - S : 0); kk < k; ++kk) tma::mbar_wait(&full[kk % S], (uint32_t)((kk / S) & 1), a.spin);
         return;
     }
 
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kNT, 2)
     int k = 0;
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
         const int stg = k % S;
-        bool ok = tma::mbar_wait(&full[stg], (uint32_t)((k / S) & 1));
+        bool ok = tma::mbar_wait(&full[stg], (uint32_t)((k / S) & 1), a.spin);
         if (T == 2) {
             // the ring tile is shared by all consumer warps: agree on going on
             if (!ok) abort_flag = 1;

@@ -80,6 +80,9 @@ struct FwdTmaArgs {
     float* out1;              // Q^{t+1}
     float* out2;              // Q^{t+2} (two-level launches)
     int* err;                 // raised when a bounded wait gives up
+    unsigned spin;            // polls of a bounded wait before it gives up
+    int stall;                // failure drill: this CTA withholds its first
+                              // tile and its grid-barrier arrival (-1: none)
 };
 
 // Cooperative multi-level forward kernel (k_fwd_loop.cu): levels
@@ -122,6 +125,8 @@ struct FwdResArgs {
     ulonglong2* xbuf;         // halo words, two (value | level << 32) halves each:
                               // [2 parities][nslab][2 sides][2 ldz], zero at launch
     int* err;
+    unsigned spin;            // polls of a bounded wait before it gives up
+    int stall;                // failure drill: this slab publishes no halo (-1: none)
 };
 
 struct FwdTmaConfig {
@@ -152,6 +157,9 @@ struct BwdLoopArgs {
     float* acc_b;
     int* err;
     unsigned* sync;           // grid-barrier counter, zero at launch
+    unsigned spin;            // polls of a bounded wait before it gives up
+    int stall;                // failure drill: this CTA withholds its first
+                              // tile and its grid-barrier arrival (-1: none)
 };
 
 struct BwdArgs {

@@ -1,8 +1,9 @@
 // tma.cuh — inline-PTX helpers for TMA tile loads and mbarriers (sm_100a).
 //
-// Every wait is bounded: try_wait loops give up after kSpinLimit polls and
-// report failure, so a kernel can raise its error flag and return instead of
-// hanging the GPU.  No load here uses .multicast::cluster.
+// Every wait is bounded: try_wait loops give up after a number of polls
+// (kSpinLimit unless the caller passes its own limit) and report failure, so a
+// kernel can raise its error flag and return instead of hanging the GPU.  No
+// load here uses .multicast::cluster.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -48,10 +49,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait on the phase with the given parity; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kSpinLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// A kernel's error flag as it stands in L2 (another CTA may have raised it).
+__device__ __forceinline__ int ld_flag(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
 __device__ __forceinline__ void prefetch_map(const CUtensorMap* m) {

@@ -22,7 +22,17 @@
 //   with them: ABC off, d_Vp replaced by vel_padded.bin (nzz x nxx), then per
 //   shot forward + RTM backward and forward + gradient backward, with the input
 //   traces of shot k read from <data_prefix><k>.bin.
+// usage: ref_harness --time <parameters.txt> <vel_padded.bin> <data_prefix> <reps>
+//   times, with CUDA events on the default stream, the reference's own loops
+//   on every shot: forward_solver (compute_pressure + compute_seismogram,
+//   modeling.cu:286-299, ABC off), the migration back-propagation
+//   (inject_seismogram + cross_correlation, migration.cu:61-81) and the
+//   adjoint back-propagation (inject_adjoint + build_gradient,
+//   inversion.cu:230-248); prints one line per repetition:
+//   "time fwd_ms=... rtm_bwd_ms=... grad_bwd_ms=... updates=..." where updates
+//   = shots x nxx x nzz x (nt + tlag) per propagation.
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -76,6 +86,72 @@ public:
         }
     }
 
+    // one back-propagation of the current source field, as the reference's loops
+    void backward_loop(int mode, float* d_Pr, float* d_Prold, float* d_acc, float* d_ill) {
+        const int nrec = geometry->nrec;
+        for (int tId = 0; tId < nt + tlag; tId++) {
+            if (mode == 0) {
+                inject_seismogram<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
+                cross_correlation<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, idh2, dt);
+            } else {
+                inject_adjoint<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
+                build_gradient<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, nt, dt, idh2);
+            }
+            std::swap(d_P, d_Pold);
+            std::swap(d_Pr, d_Prold);
+        }
+    }
+
+    void time_loops(const std::string& params, const char* vel_file, const char* data_prefix, int reps) {
+        parameters = params;
+        set_parameters();
+        ABC = false;
+        const int nrec = geometry->nrec;
+        std::vector<float> v = load(vel_file, (size_t)matsize);
+        cudaMemcpy(d_Vp, v.data(), matsize * sizeof(float), cudaMemcpyHostToDevice);
+        float *d_Pr = nullptr, *d_Prold = nullptr, *d_acc = nullptr, *d_ill = nullptr;
+        cudaMalloc(&d_Pr, matsize * sizeof(float));
+        cudaMalloc(&d_Prold, matsize * sizeof(float));
+        cudaMalloc(&d_acc, matsize * sizeof(float));
+        cudaMalloc(&d_ill, matsize * sizeof(float));
+        std::vector<std::vector<float>> data(geometry->nsrc);
+        for (int s = 0; s < geometry->nsrc; ++s)
+            data[s] = load(std::string(data_prefix) + std::to_string(s + 1) + ".bin", (size_t)nt * nrec);
+        cudaEvent_t e[2];
+        cudaEventCreate(&e[0]);
+        cudaEventCreate(&e[1]);
+        auto timed = [&](auto&& fn) {
+            cudaEventRecord(e[0]);
+            fn();
+            cudaEventRecord(e[1]);
+            cudaEventSynchronize(e[1]);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e[0], e[1]);
+            return (double)ms;
+        };
+        for (int r = 0; r < reps; ++r) {
+            double fwd = 0, rtm = 0, grad = 0;
+            for (srcId = 0; srcId < geometry->nsrc; srcId++) {
+                initialization();
+                for (int mode = 0; mode < 2; ++mode) {
+                    fwd += timed([&] { forward_solver(); });
+                    cudaMemcpy(d_seismogram, data[srcId].data(), data[srcId].size() * sizeof(float),
+                               cudaMemcpyHostToDevice);
+                    cudaMemset(d_Pr, 0, matsize * sizeof(float));
+                    cudaMemset(d_Prold, 0, matsize * sizeof(float));
+                    cudaMemset(d_acc, 0, matsize * sizeof(float));
+                    cudaMemset(d_ill, 0, matsize * sizeof(float));
+                    (mode == 0 ? rtm : grad) += timed([&] { backward_loop(mode, d_Pr, d_Prold, d_acc, d_ill); });
+                }
+            }
+            cudaError_t err = cudaDeviceSynchronize();
+            if (err != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); std::exit(3); }
+            std::printf("time fwd_ms=%.4f rtm_bwd_ms=%.4f grad_bwd_ms=%.4f updates=%lld\n", fwd / 2, rtm, grad,
+                        (long long)geometry->nsrc * nxx * nzz * (nt + tlag));
+            std::fflush(stdout);
+        }
+    }
+
     void run(const std::string& params, const std::string& out, const char* vel_file, const char* data_prefix) {
         parameters = params;
         set_parameters();
@@ -114,17 +190,7 @@ public:
                 cudaMemset(d_Prold, 0, matsize * sizeof(float));
                 cudaMemset(d_acc, 0, matsize * sizeof(float));
                 cudaMemset(d_ill, 0, matsize * sizeof(float));
-                for (int tId = 0; tId < nt + tlag; tId++) {
-                    if (mode == 0) {
-                        inject_seismogram<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
-                        cross_correlation<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, idh2, dt);
-                    } else {
-                        inject_adjoint<<<sBlocks, NTHREADS>>>(d_Pr, d_rIdx, d_rIdz, d_seismogram, nrec, tId, nt, nzz, idh2);
-                        build_gradient<<<nBlocks, NTHREADS>>>(d_P, d_Pold, d_Pr, d_Prold, d_Vp, d_acc, d_ill, nxx, nzz, nt, dt, idh2);
-                    }
-                    std::swap(d_P, d_Pold);
-                    std::swap(d_Pr, d_Prold);
-                }
+                backward_loop(mode, d_Pr, d_Prold, d_acc, d_ill);
                 const char* tag = mode == 0 ? "image" : "grad";
                 save(out + "/" + tag + "_" + k + ".bin", d_acc, matsize);
                 save(out + "/" + tag + "_illum_" + k + ".bin", d_ill, matsize);
@@ -137,6 +203,11 @@ public:
 };
 
 int main(int argc, char** argv) {
+    if (argc == 6 && std::string(argv[1]) == "--time") {
+        Driver d;
+        d.time_loops(argv[2], argv[3], argv[4], std::atoi(argv[5]));
+        return 0;
+    }
     if (argc != 3 && argc != 5) {
         std::fprintf(stderr, "usage: %s parameters.txt outdir [vel_padded.bin data_prefix]\n", argv[0]);
         return 1;
