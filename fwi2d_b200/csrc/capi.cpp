@@ -366,6 +366,7 @@ int fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, s
     std::string err;
     int rc = fwi::residual_noalloc(d_obs, d_cal, d_res, n, d_sum, static_cast<cudaStream_t>(stream), &err);
     if (rc != FWI_OK) g_create_error = err;
+    else g_create_error.clear();  // no stale message after a call that succeeded
     return rc;
 }
 

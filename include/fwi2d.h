@@ -231,9 +231,16 @@ int  fwi_util_normal(uint64_t seed, uint32_t shot, uint32_t stream, uint64_t ctr
  * (d_sum: one double); `stream` is a cudaStream_t (NULL: default stream) and
  * the call only enqueues work.  The scratch is a 64 KiB file-scope device
  * array, so n is limited to FWI_NOALLOC_MAX_SAMPLES (FWI_ERR_ARG beyond it;
- * split larger inputs).  The first call on a device looks the array up, so
- * make it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * split larger inputs).  The first call on a device looks the array's device
+ * address up (cudaGetSymbolAddress, which may load the library's device code
+ * at that moment under CUDA's lazy module loading), so make it before any
+ * stream capture.  The address is kept per device ordinal for the life of
+ * the process: after cudaDeviceReset, or anything else that destroys the
+ * device's primary context, it is stale and the entry point must not be
+ * called again in that process.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  A failed
+ * call leaves its message for fwi_last_error(NULL); a call that succeeds
+ * clears it. */
 #define FWI_NOALLOC_MAX_SAMPLES ((size_t)8192 * 8192)
 int  fwi_residual_noalloc(const float* d_obs, const float* d_cal, float* d_res, size_t n, double* d_sum,
                           void* stream);

@@ -389,6 +389,17 @@ static int o_pds(float x_max, float z_max, float radius, uint64_t seed, uint32_t
     return np;
 }
 
+/* The raw point set of one shot's sampler, before the band filter of
+ * set_random_boundary: (x, z) pairs into out; returns the count (at most cap
+ * are written). */
+int orc_pds(float x_max, float z_max, float radius, uint64_t seed, uint32_t shot, float* out, int cap) {
+    OPt* pts = (OPt*)malloc(sizeof(OPt) * (size_t)(cap > 0 ? cap : 1));
+    int np = o_pds(x_max, z_max, radius, seed, shot, pts, cap);
+    for (int k = 0; k < np && k < cap; k++) { out[2 * k] = pts[k].x; out[2 * k + 1] = pts[k].z; }
+    free(pts);
+    return np;
+}
+
 /* Bumps of one shot: (xc, zc, r, A, factor) x count into out (5 floats each). */
 int orc_bumps(int nxx, int nzz, int nb, float dh, float ratio, float varVp, uint64_t seed, uint32_t shot,
               float* out, int cap) {

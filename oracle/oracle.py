@@ -59,6 +59,8 @@ def _lib(bits: int = 64) -> C.CDLL:
         lib.orc_bumps.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_uint32,
                                   _F, C.c_int]
         lib.orc_bumps.restype = C.c_int
+        lib.orc_pds.argtypes = [C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_uint32, _F, C.c_int]
+        lib.orc_pds.restype = C.c_int
         lib.orc_rbc.argtypes = [_F, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint64,
                                 C.c_uint32, _F, C.c_int, _F]
         lib.orc_ppnd16.argtypes = [C.c_double]
@@ -216,6 +218,15 @@ def backward(vel: np.ndarray, data: np.ndarray, nt: int, tlag: int, dt: float, d
 # ----------------------------------------------------------- random boundary
 def normal(seed: int, shot: int, stream: int, ctr: int) -> float:
     return float(_lib().orc_normal(seed, shot, stream, ctr))
+
+
+def pds(x_max: float, z_max: float, radius: float, seed: int, shot: int) -> np.ndarray:
+    """The seeded Poisson-disk point set (n, 2) of (x, z) before the band filter."""
+    cap = 1 << 20
+    out = np.empty(2 * cap, np.float32)
+    n = _lib().orc_pds(x_max, z_max, radius, seed, shot, _f(out), cap)
+    assert n <= cap
+    return out[: 2 * n].reshape(-1, 2)
 
 
 def bumps(nxx, nzz, nb, dh, ratio, varVp, seed, shot) -> np.ndarray:

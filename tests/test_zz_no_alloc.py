@@ -8,8 +8,11 @@ device array shared by all calls.  This test calls it through the C ABI on
 device buffers and compares it with the existing entry point,
 fwi_compute_gradient, whose misfit reduction uses context-allocated scratch:
 two calls in a row on different data, each within the tolerance of the other
-GPU tests (relative 1e-4), and the residual bit for bit.  The file sorts last
-so a run stopped at the first failure has run every other test already.
+GPU tests (relative 1e-4), and the residual bit for bit.  The chunk edges of
+the scratch (8192 samples a partial sum) are checked against numpy's FP64 sum
+of squares: no sample, exactly one chunk, and a partial last chunk.  The file
+sorts last so a run stopped at the first failure has run every other test
+already.
 """
 import ctypes as C
 
@@ -68,3 +71,28 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                         C.c_void_p(t.data_ptr()), 8192 * 8192 + 1, C.c_void_p(s.data_ptr()), None)
     assert rc == -8
     assert b"exceeds the maximum" in api.lib().fwi_last_error(None)
+
+
+@pytest.mark.parametrize("n", [0, 8192, 3 * 8192 + 5])
+def test_noalloc_chunk_edges_vs_numpy(n):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(n)
+    obs = rng.standard_normal(max(n, 1)).astype(np.float32)
+    cal = rng.standard_normal(max(n, 1)).astype(np.float32)
+    d_obs, d_cal = torch.from_numpy(obs).to(dev), torch.from_numpy(cal).to(dev)
+    d_res = torch.full((max(n, 1),), np.nan, dtype=torch.float32, device=dev)
+    d_sum = torch.full((1,), np.nan, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    assert _noalloc(d_obs, d_cal, d_res, n, d_sum) == 0, api.lib().fwi_last_error(None)
+    assert api.lib().fwi_last_error(None) == b""
+    torch.cuda.synchronize()
+    res = (obs[:n] - cal[:n]).astype(np.float32)
+    ref = float(np.sum(res.astype(np.float64) ** 2))
+    got = float(d_sum.item())
+    if n == 0:
+        assert got == 0.0
+    else:
+        assert abs(got - ref) <= 1e-12 * ref, (n, got, ref)
+        assert np.array_equal(d_res[:n].cpu().numpy(), res)
