@@ -118,6 +118,7 @@ private:
         int* d_rec_colptr = nullptr;       // nsrc*(nxx+1)
         int* d_rec_z = nullptr;            // nsrc*nrec, sorted by column
         long long* d_rec_soff = nullptr;
+        RecCol* d_rec_col = nullptr;       // per shot column: receivers there (first one's row, trace)
         std::vector<int> h_src_colptr, h_rec_colptr;  // host copies of the column tables
     };
     enum Kind { kFwdRecord = 0, kFwdNoRecord = 1, kBwdImage = 2, kBwdGradient = 3 };

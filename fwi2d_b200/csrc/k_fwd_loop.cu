@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(kNT, MINB)
                     mt.col_off = sd.col_off;
                     mt.has_src = a.sample1 >= 0 &&
                                  st::has_points(a.inj, sd.col_off, ti.x0, min(ti.x0 + TX, sd.nxx));
-                    if (a.rec_sample0 >= 0 && a.seis) {
+                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
+                    if (a.rec_sample0 >= 0 && a.seis && ti.z0 <= sd.rec_zmax && ti.z0 + kTZ > sd.rec_zmin) {
                         mt.rec_kb = __ldg(a.rec.colptr + sd.col_off + ti.x0);
                         mt.rec_ke = __ldg(a.rec.colptr + sd.col_off + min(ti.x0 + TX, sd.nxx));
                     } else {
@@ -156,21 +157,23 @@ __global__ void __launch_bounds__(kNT, MINB)
                 tl.has_src = mt.has_src != 0;
                 const float* b1d = ABC ? a.b1d : nullptr;
                 if (mt.rec_kb < mt.rec_ke) {
+                    // one thread per column of the tile: the column's receivers
+                    // from the per-column table (one load), more than one
+                    // receiver in a column from the column table
                     const int xe = min(tl.ti.x0 + TX, tl.nxx);
-                    for (int r = mt.rec_kb + tid; r < mt.rec_ke; r += kNC) {
-                        const int z = __ldg(a.rec.z + r);
-                        if (z < tl.ti.z0 || z >= tl.ti.z0 + kTZ) continue;
-                        int lo = tl.ti.x0, hi = xe;
-                        while (hi - lo > 1) {
-                            const int m = (lo + hi) >> 1;
-                            if (__ldg(a.rec.colptr + tl.col_off + m) <= r) lo = m;
-                            else hi = m;
+                    for (int x = tl.ti.x0 + tid; x < xe; x += kNC) {
+                        const int4 rc = __ldg(reinterpret_cast<const int4*>(a.rec_col + tl.col_off + x));
+                        const int kb = rc.y > 1 ? __ldg(a.rec.colptr + tl.col_off + x) : 0;
+                        for (int q = 0; q < rc.y; ++q) {
+                            const int z = q == 0 ? rc.x : __ldg(a.rec.z + kb + q);
+                            if (z < tl.ti.z0 || z >= tl.ti.z0 + kTZ) continue;
+                            const long long soff = q == 0 ? (((long long)(unsigned)rc.w << 32) | (unsigned)rc.z)
+                                                          : __ldg(a.rec.soff + kb + q);
+                            const float d = ABC ? st::damp(st::rows_info(a.b1d, a.nb, z, a.nzz),
+                                                           st::col_info(a.b1d, a.nb, x, tl.nxx), 0)
+                                                : 1.0f;
+                            a.seis[soff + a.rec_sample0] = d * tl.cur[(x - tl.ti.x0 + 4) * G::CZ + (z - tl.ti.z0 + 4)];
                         }
-                        const float d = ABC ? st::damp(st::rows_info(a.b1d, a.nb, z, a.nzz),
-                                                       st::col_info(a.b1d, a.nb, lo, tl.nxx), 0)
-                                            : 1.0f;
-                        a.seis[__ldg(a.rec.soff + r) + a.rec_sample0] =
-                            d * tl.cur[(lo - tl.ti.x0 + 4) * G::CZ + (z - tl.ti.z0 + 4)];
                     }
                 }
                 const bool inner = st::tile_inner(tl.ti.z0, kTZ, tl.ti.x0, TX, a.nzz, tl.nxx);

@@ -28,6 +28,16 @@ struct ShotDesc {
     long long seis_off;  // float offset of the shot's nt x nrec trace-major block
     int vel_col;         // column of the velocity array that is column 0 of the
                          // shot's grid (aperture window over a shared velocity)
+    int rec_zmin, rec_zmax;  // rows of the shot's receivers (zmin > zmax: none)
+};
+
+// Receivers of one grid column of a shot (entry col_off + x, as the receiver
+// column table): how many, and the row and trace offset of the first.  The
+// back-propagation kernel reads it instead of walking the column table.
+struct __align__(16) RecCol {
+    int z;
+    int n;
+    long long soff;
 };
 
 // Point injections into the field written by a step (the source of a forward
@@ -75,6 +85,7 @@ struct FwdTmaArgs {
     InjTable inj;             // source table; sample1 / sample2 below
     int sample1, sample2;     // wavelet samples added to Q^{t+1}, Q^{t+2}; -1 none
     InjTable rec;             // receiver table (colptr, z, soff) of the batch
+    const RecCol* rec_col;    // per-column receivers (indexed like rec.colptr)
     float* seis;              // trace-major seismograms, NULL when not recording
     int rec_sample0, rec_sample1;  // samples recorded from Q^t and Q^{t+1}; -1 none
     float* out1;              // Q^{t+1}
@@ -155,6 +166,7 @@ struct BwdLoopArgs {
     float* pr[2];
     float* acc_a;
     float* acc_b;
+    const RecCol* rec_col;    // per-column receivers (indexed like inj.colptr)
     int* err;
     unsigned* sync;           // grid-barrier counter, zero at launch
     unsigned spin;            // polls of a bounded wait before it gives up

@@ -107,7 +107,11 @@ def line_search(ctx: api.Context, f0: float, cap: float | None = STEP_CAP) -> tu
     return step, f1, f2
 
 
-def make_pairs(root, models: int, stages: int = 4, seed0: int = 1000, setup: PairSetup = PairSetup(), log=print):
+TRAIN_SEED0 = 1000  # training models use seeds TRAIN_SEED0 ..; test models use seeds below it
+
+
+def make_pairs(root, models: int, stages: int = 4, seed0: int = TRAIN_SEED0, setup: PairSetup = PairSetup(),
+               log=print):
     """models x stages pairs -> (X: [n, P*16] bf16, T: [n, P] float32) on the device.
     Stage k of a model is its k-th plain-FWI iterate from the 1-D start."""
     torch = _torch()

@@ -5,7 +5,10 @@ made by the FD engine on seeded dipping-layer models, the U-Net trained on
 them with the project's kernels, then FWI of a held-out model from the same
 1-D start, plain and CNN-preconditioned (fallback to the gradient when the
 line search along the network's direction does not cut the misfit).  The
-network must cut the data misfit faster than the gradient does."""
+network must cut the data misfit faster than the gradient does, and it must
+reach a lower model error than the plain run reaches, in less wall time (the
+quantity the preconditioner is judged on: model RMS error against time).  The
+training models are held out from the test model (different seeds)."""
 import numpy as np
 import pytest
 
@@ -53,3 +56,19 @@ def test_cnn_direction_cuts_misfit_faster(trained):
     # residuo[k] is the misfit before update k + 1: compare after two updates
     assert cnn_run.residuo[-1] < plain.residuo[-1], (cnn_run.residuo, plain.residuo)
     assert all(np.isfinite(cnn_run.model_error))
+    # model error against wall time: the CNN run gets below the plain run's
+    # best error, and gets there before the plain run has finished
+    best_plain = min(plain.model_error)
+    t_cnn = precond.time_to_error(cnn_run, best_plain * 0.999)
+    print(f"\n[precond] model error plain {plain.model_error} ({plain.seconds[-1]:.2f} s), "
+          f"cnn {cnn_run.model_error} ({cnn_run.seconds[-1]:.2f} s)")
+    assert t_cnn is not None, (plain.model_error, cnn_run.model_error)
+    assert t_cnn < plain.seconds[-1], (t_cnn, plain.seconds)
+
+
+def test_training_models_are_held_out():
+    """The pairs come from seeds TRAIN_SEED0 .. TRAIN_SEED0 + models - 1; the
+    FWI test models (seeds 7 and 11 here, the 301 x 1701 model of seed 2 in
+    the survey experiment) are none of them."""
+    for seed in (2, 7, 11):
+        assert not (precond.TRAIN_SEED0 <= seed < precond.TRAIN_SEED0 + 4096)
