@@ -10,8 +10,9 @@
 //   * per tap, the 128 threads stage A_tap (128 x Cin) and B_tap (Cout x Cin)
 //     in shared memory in the canonical K-major layout without swizzle
 //     (8-row x 16-byte core matrices; K-adjacent core matrices 128 B apart,
-//     8-row groups Cin/8 x 128 B apart), two stages so the loads of tap t+1
-//     overlap the MMAs of tap t;
+//     8-row groups Cin/8 x 128 B apart) with 16-byte cp.async copies (zero
+//     fill outside the image), all of a tap's copies in flight at once, two
+//     stages so the copies of tap t+1 overlap the MMAs of tap t;
 //   * one thread issues the tap's Cin/16 `tcgen05.mma.cta_group::1.kind::f16`
 //     (BF16 x BF16 -> FP32, M = 128, N = Cout) into a TMEM accumulator and
 //     commits them to the stage's mbarrier;
@@ -71,13 +72,25 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t r[8]) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(addr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 16-byte asynchronous copy global -> shared memory (L2 only); src_bytes 0
+// writes zeros (the source address must still be a valid one).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+// Wait for every cp.async of the thread, then make the copies visible to the
+// tensor cores' (async proxy) reads.
+__device__ __forceinline__ void cp_async_wait_all_async_proxy() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -136,16 +149,14 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
         const uint4* src = reinterpret_cast<const uint4*>(in + (((long long)n * H + (in_ok ? yy : 0)) * W +
                                                                 (in_ok ? xx : 0)) * Cin);
         unsigned char* arow = A + (size_t)(tid >> 3) * kc * 128 + (tid & 7) * 16;
-        for (int j = 0; j < kc; ++j) {
-            const uint4 v = in_ok ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
-            *reinterpret_cast<uint4*>(arow + (size_t)j * 128) = v;
-        }
+        const uint32_t a_src = in_ok ? 16u : 0u;
+        for (int j = 0; j < kc; ++j) cp_async16(arow + (size_t)j * 128, src + j, a_src);
         for (int e = tid; e < Cout * kc; e += kTcThreads) {
             const int co = e / kc, j = e - co * kc;
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + ((long long)co * 9 + tap) * Cin) + j);
-            *reinterpret_cast<uint4*>(B + ((size_t)(co >> 3) * kc + j) * 128 + (co & 7) * 16) = v;
+            cp_async16(B + ((size_t)(co >> 3) * kc + j) * 128 + (co & 7) * 16,
+                       reinterpret_cast<const uint4*>(w + ((long long)co * 9 + tap) * Cin) + j, 16u);
         }
-        fence_async_smem();  // the tensor cores read these stores through the async proxy
+        cp_async_wait_all_async_proxy();  // the tensor cores read these copies through the async proxy
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
@@ -246,28 +257,31 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
         unsigned char* B = A + a_bytes;
         if (st >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((st - 2) >> 1) & 1))) ok = false;
         const long long q0 = p_begin + (long long)st * kWgK;
-        // A: dout rows (pixels) x co, 16 co groups x 64 pixels
+        // A: dout rows (pixels) x co, 16 co groups x 64 pixels (zeros past the
+        // chunk and past Cout; the copy's source is then pixel p_begin, channel 0)
         for (int e = tid; e < 16 * kWgK; e += kTcThreads) {
             const int mi = e / kWgK, r = e - mi * kWgK;  // co group, pixel in stage
             const long long q = q0 + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (q < p_end && mi * 8 < Cout) v = __ldg(reinterpret_cast<const uint4*>(dout + q * Cout + mi * 8));
-            *reinterpret_cast<uint4*>(A + ((size_t)mi * 8 + (r >> 3)) * 128 + (r & 7) * 16) = v;
+            const bool ok_a = q < p_end && mi * 8 < Cout;
+            cp_async16(A + ((size_t)mi * 8 + (r >> 3)) * 128 + (r & 7) * 16,
+                       reinterpret_cast<const uint4*>(dout + (ok_a ? q * Cout + mi * 8 : p_begin * Cout)),
+                       ok_a ? 16u : 0u);
         }
-        // B: shifted input rows (pixels) x ci
+        // B: shifted input rows (pixels) x ci (zeros outside the image)
         for (int e = tid; e < nci * kWgK; e += kTcThreads) {
             const int ni = e / kWgK, r = e - ni * kWgK;
             const long long q = q0 + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            bool ok_b = false;
             if (q < p_end) {
                 const int x = (int)(q % W);
                 const int y = (int)((q / W) % H);
-                if (x + dx >= 0 && x + dx < W && y + dy >= 0 && y + dy < H)
-                    v = __ldg(reinterpret_cast<const uint4*>(in + (q + (long long)dy * W + dx) * Cin + ni * 8));
+                ok_b = x + dx >= 0 && x + dx < W && y + dy >= 0 && y + dy < H;
             }
-            *reinterpret_cast<uint4*>(B + ((size_t)ni * 8 + (r >> 3)) * 128 + (r & 7) * 16) = v;
+            cp_async16(B + ((size_t)ni * 8 + (r >> 3)) * 128 + (r & 7) * 16,
+                       reinterpret_cast<const uint4*>(in + (ok_b ? (q + (long long)dy * W + dx) * Cin + ni * 8 : 0)),
+                       ok_b ? 16u : 0u);
         }
-        fence_async_smem();
+        cp_async_wait_all_async_proxy();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();

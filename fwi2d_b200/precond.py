@@ -252,6 +252,9 @@ def fwi(ctx: api.Context, v_true: np.ndarray, iterations: int, net: cnn.UNet | N
     return out
 
 
+THRESHOLDS = (0.12, 0.11, 0.10, 0.09, 0.08, 0.07, 0.06, 0.05, 0.04, 0.03)  # relative model RMS error
+
+
 def time_to_error(log: FwiLog, target: float) -> float | None:
     """Seconds until the model error first reaches `target` (None if never)."""
     for e, t in zip(log.model_error[1:], log.seconds):
@@ -320,7 +323,8 @@ def main(argv=None) -> int:
             ctx.set_seed(7)
             lg = fwi(ctx, vt, a.iterations, net if mode == "cnn" else None)
             runs[mode] = {"residuo": lg.residuo, "model_error": lg.model_error, "seconds": lg.seconds,
-                          "direction": lg.direction, "time_to_target": time_to_error(lg, a.target)}
+                          "direction": lg.direction, "time_to_target": time_to_error(lg, a.target),
+                          "time_to": {f"{t:.3f}": time_to_error(lg, t) for t in THRESHOLDS}}
     res["runs"] = runs
     txt = json.dumps(res)
     if a.out:
