@@ -329,13 +329,19 @@ def rtm_benchmark_geometry(reps: int = 2) -> dict:
     return out
 
 
+FWI_VMIN, FWI_VMAX = 1400.0, 4800.0  # bounds of the FWI companion's velocity update (m/s)
+
+
 def fwi_measure(case, vp_true: np.ndarray, iterations: int) -> dict:
     """The reference's FWI iteration (inversion_main.cpp:13-22: compute_gradient,
     optimization = two line-search modelings + the parabola, update_model;
     inversion.cu:111-358) from the 1-D depth-gradient model, through the C ABI;
-    observed data modeled in the true model by the same engine.  Reports the
-    wall time per iteration and the misfit and relative model RMS error after
-    each."""
+    observed data modeled in the true model by the same engine.  The update is
+    the reference's parabola step with the velocity bounded to [FWI_VMIN,
+    FWI_VMAX] (fwi_update_model_bounded): the reference's unbounded update
+    made the 81-shot survey's model unstable at its 4th iteration (non-finite
+    misfit at the 5th).  Reports the wall time per iteration and the misfit
+    and relative model RMS error after each."""
     import torch
 
     from fwi2d_b200 import api, synth
@@ -357,11 +363,12 @@ def fwi_measure(case, vp_true: np.ndarray, iterations: int) -> dict:
             sum_res = ctx.compute_gradient(True)
             f0 = float(np.sqrt(np.float32(sum_res)))
             step = ctx.optimization(f0)
-            v = ctx.update_model(step)
+            v = ctx.update_model_bounded(step, FWI_VMIN, FWI_VMAX)
             res["seconds"].append(time.perf_counter() - t0)
             res["misfit"].append(f0)
             res["step"].append(float(step))
             res["model_error"].append(err(v))
+        res["update"] = f"the reference's parabola step, velocity bounded to [{FWI_VMIN:g}, {FWI_VMAX:g}] m/s"
         res["s_per_iteration"] = float(np.mean(res["seconds"]))
         res["shots_per_s"] = dims.nsrc / res["s_per_iteration"]
         res["plans"] = ctx.describe()

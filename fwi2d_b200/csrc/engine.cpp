@@ -1687,6 +1687,9 @@ double Engine::accumulate_gradient(bool with_gradient) {
     }
     if (with_gradient) ++rbc_epoch_;
     sync("accumulate_gradient");
+    if (!std::isfinite(sum))
+        throw Error(FWI_ERR_NAN, "accumulate_gradient: non-finite misfit (the model's propagation is unstable: a "
+                                 "velocity above the CFL limit or a non-positive slowness^2 after an update?)");
     return sum;
 }
 

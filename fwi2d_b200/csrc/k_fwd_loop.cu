@@ -33,8 +33,9 @@ namespace {
 
 using namespace ft;
 
-// Gives up after `limit` polls, or at once when another CTA has raised *err
-// (that CTA has left the level loop and will never arrive).
+// Gives up after `limit` polls, or when another CTA has raised *err (that CTA
+// has left the level loop and will never arrive; checked every 32nd poll so
+// that the flag's load does not slow the barrier).
 __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, uint32_t limit, const int* err) {
     __threadfence();
     atomicAdd(counter, 1u);
@@ -42,7 +43,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
         if (v >= target) return true;
-        if (tma::ld_flag(err)) return false;
+        if ((i & 31u) == 31u && tma::ld_flag(err)) return false;  // every 32nd poll only
         __nanosleep(64);
     }
     return false;

@@ -39,9 +39,10 @@
 // before every launch (level 0 is no level).  Every wait is bounded
 // (a.spin polls); a wait that gives up raises *err and the CTA leaves the
 // level loop (with no asynchronous copy in flight and its TMEM released).  A
-// poll also gives up as soon as *err is raised, so one failure ends every
-// slab's level loop at its next missing halo word instead of slab after slab
-// through each one's own timeout.  The failure drill (a.stall) makes one slab
+// poll also gives up once *err is raised (checked every 32nd poll, so the
+// flag's load does not slow the polling), so one failure ends every slab's
+// level loop at its next missing halo word instead of slab after slab through
+// each one's own timeout.  The failure drill (a.stall) makes one slab
 // publish no halo words, so its neighbours' polls run out.
 #include <cuda_runtime.h>
 
@@ -523,7 +524,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
                             ok = true;
                             break;
                         }
-                        if (tma::ld_flag(a.err)) break;
+                        if ((spin & 31u) == 31u && tma::ld_flag(a.err)) break;  // every 32nd poll only
                         __nanosleep(64);
                     }
                 }
