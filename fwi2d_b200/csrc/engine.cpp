@@ -900,7 +900,9 @@ void Engine::launch_fwd_res_levels(const FwdPlan& p, const Grid& g, const Tables
                                    const float* in_old, float* out_cur, float* out_old, int t_begin, int t_end,
                                    long long timed_updates) {
     const size_t nsl = p.slabs.size();
-    const size_t xb = (size_t)8 * nsl * g.ldz;  // 16-byte words: 2 parities x 2 sides x 2 ldz per slab
+    // 16-byte words: 2 parities x 2 sides x 2 ldz per slab, and one slab's
+    // worth more (the failure drill's stalled slab publishes there)
+    const size_t xb = (size_t)8 * (nsl + 1) * g.ldz;
     if (nsl > slabs_cap_ || xb > xbuf_cap_) {
         check(cudaStreamSynchronize(st_), "sync before resident-kernel tables");
         cudaFree(d_slabs_);

@@ -52,10 +52,18 @@ struct BGeom {
     static constexpr uint32_t BYTES = STAGE * 4;
     static_assert((ST * 4) % 128 == 0 && (PT * 4) % 128 == 0, "TMA destinations must stay 128-byte aligned");
     static_assert(CZ <= 256 && CX <= 256, "TMA box extent");
+    static_assert(TX <= 16, "per-column receiver metadata holds 16 columns");
 };
 
+// Stage metadata, written by the producer warp before the stage's second
+// arrival.  For a tile with receivers (has_rec) the producer's lanes also
+// fetch, per tile column, the row of its receiver in the tile (-1: none) and
+// the injected amplitude of this level; multi: a column holds more than one
+// receiver, the consumers then walk the column table themselves.
 struct BMeta {
-    int s, x0, z0, nxx, col_off, has_rec;
+    int s, x0, z0, nxx, col_off, has_rec, multi;
+    int zrow[16];
+    float amp[16];
 };
 
 // Gives up after `limit` polls, or when another CTA has raised *err (that CTA
@@ -113,15 +121,6 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
     const float* t_b = t_v + 4 * G::PT;
     const st::Rows rows = st::rows_info(nullptr, 0, z, a.nzz);
     const int c0 = warp * CPW;
-    // the receivers of the thread's columns, fetched before the stencil so
-    // that the load's latency hides behind the shared-memory work
-    int4 rc[CPW];
-#pragma unroll
-    for (int m = 0; m < CPW; ++m) {
-        rc[m] = make_int4(0, 0, 0, 0);
-        if (mt.has_rec && mt.x0 + c0 + m < mt.nxx)
-            rc[m] = __ldg(reinterpret_cast<const int4*>(a.rec_col + mt.col_off + mt.x0 + c0 + m));
-    }
     float ls[CPW][4], lr[CPW][4];
     float4 psold[CPW], pr[CPW];
     st::lap_run<G::CZ, CPW>(t_ps, 4 * lane + 4, c0 + 4, ls, psold);
@@ -143,18 +142,16 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
                                                        a.dt2idh2, a.dt, a.idh2, rows, colok);
         float4 rv = r.pr;
         if (mt.has_rec) {
-            // rc = {row, count, trace offset}: one receiver in the column is
-            // added here; columns with more take the column-table walk
-            const int dz = rc[m].x - z;
-            if (rc[m].y == 1 && dz >= 0 && dz < 4) {
-                const long long soff = ((long long)(unsigned)rc[m].w << 32) | (unsigned)rc[m].z;
-                const float amp = a.inj.scale * __ldg(a.inj.series + soff + sample);
+            if (mt.multi) {
+                st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
+            } else {
+                // the producer fetched this column's receiver row and amplitude
+                const int dz = mt.zrow[c] - z;
+                const float amp = mt.amp[c];
                 if (dz == 0) rv.x += amp;
                 else if (dz == 1) rv.y += amp;
                 else if (dz == 2) rv.z += amp;
-                else rv.w += amp;
-            } else if (rc[m].y > 1) {
-                st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
+                else if (dz == 3) rv.w += amp;
             }
         }
         const size_t g = so + (size_t)gx * a.ldz + z;
@@ -180,7 +177,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
 
     if (tid == 0) {
         for (int k = 0; k < S; ++k) {
-            tma::mbar_init(&full[k], 1);
+            tma::mbar_init(&full[k], 2);  // the loads' transaction bytes + the metadata arrival
             tma::mbar_init(&empty[k], kNC / 32);
         }
         abort_flag = 0;
@@ -198,29 +195,36 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
         const int sample = (b + 1 < a.nt) ? a.nt - 1 - (b + 1) : -1;
         bool ok = true;
         if (tid >= kNC) {
-            // ---------- producer: lane 0 streams this level's tiles
-            if (lane == 0) {
-                fence_proxy_async_global();
-                int kk = k;
-                for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
-                    const int stg = kk % S;
-                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), a.spin)) {
-                        ok = false;
-                        break;
-                    }
-                    if (a.stall == (int)blockIdx.x && b == a.b_begin && kk == k) continue;  // failure drill
-                    const ft::TileInfo ti = decode_tile(a, tile, TX);
-                    const int s = ti.s, z0 = ti.z0, x0 = ti.x0;
-                    const ShotDesc sd = a.shots[s];
-                    BMeta& mt = meta[stg];
+            // ---------- producer warp: lane 0 streams this level's tiles with
+            // TMA; for tiles with receivers all lanes then fetch the level's
+            // amplitudes into the stage metadata, and lane 0 adds the stage's
+            // second arrival once they are written
+            if (lane == 0) fence_proxy_async_global();
+            int kk = k;
+            for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
+                const int stg = kk % S;
+                bool free_stage = true;
+                if (lane == 0 && kk >= S)
+                    free_stage = tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), a.spin);
+                if (!__shfl_sync(0xffffffffu, free_stage, 0)) {
+                    ok = false;
+                    break;
+                }
+                if (a.stall == (int)blockIdx.x && b == a.b_begin && kk == k) continue;  // failure drill
+                const ft::TileInfo ti = decode_tile(a, tile, TX);
+                const int s = ti.s, z0 = ti.z0, x0 = ti.x0;
+                const ShotDesc sd = a.shots[s];
+                BMeta& mt = meta[stg];
+                // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
+                const bool rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
+                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
+                if (lane == 0) {
                     mt.s = s;
                     mt.x0 = x0;
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
-                    mt.has_rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
-                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
+                    mt.has_rec = rec;
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
@@ -231,12 +235,36 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     tma::load_3d(pts + 2 * G::PT, &maps.pr_pt[p], z0, x0, s, &full[stg]);
                     tma::load_3d(pts + 3 * G::PT, &maps.acc_a, z0, x0, s, &full[stg]);
                     tma::load_3d(pts + 4 * G::PT, &maps.acc_b, z0, x0, s, &full[stg]);
+                }
+                if (rec) {
+                    // lane j: column x0 + j; rc = {row, count, trace offset of the first}
+                    int zr = -1, many = 0;
+                    float amp = 0.0f;
+                    if (lane < TX && x0 + lane < sd.nxx) {
+                        const int4 rc = __ldg(reinterpret_cast<const int4*>(a.rec_col + sd.col_off + x0 + lane));
+                        many = rc.y > 1;
+                        if (rc.y == 1 && rc.x >= z0 && rc.x < z0 + kTZ) {
+                            const long long soff = ((long long)(unsigned)rc.w << 32) | (unsigned)rc.z;
+                            zr = rc.x;
+                            amp = a.inj.scale * __ldg(a.inj.series + soff + sample);
+                        }
+                    }
+                    const unsigned multi = __ballot_sync(0xffffffffu, many);
+                    if (lane < TX) {
+                        mt.zrow[lane] = zr;
+                        mt.amp[lane] = amp;
+                    }
+                    if (lane == 0) mt.multi = multi != 0u;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    tma::mbar_arrive(&full[stg]);  // the metadata is complete
                     issued = kk + 1;
                 }
-                if (!ok) {
-                    atomicExch(a.err, 1);
-                    abort_flag = 1;
-                }
+            }
+            if (!ok && lane == 0) {
+                atomicExch(a.err, 1);
+                abort_flag = 1;
             }
         } else {
             // ---------- consumers
@@ -251,7 +279,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     ok = false;
                     break;
                 }
-                const BMeta mt = meta[stg];
+                const BMeta& mt = meta[stg];  // read in place: rewritten only after this stage is released
                 const float* stage = smem + stg * G::STAGE;
                 if (st::tile_inner(mt.z0, kTZ, mt.x0, TX, a.nzz, mt.nxx))
                     bwd_tile<TX, GRAD, false>(a, stage, mt, sample, ps_out, pr_out);

@@ -37,13 +37,16 @@
 // parity slot two levels later, after it has read its neighbours' next
 // level, which they published only after reading that slot.  It is zeroed
 // before every launch (level 0 is no level).  Every wait is bounded
-// (a.spin polls); a wait that gives up raises *err and the CTA leaves the
-// level loop (with no asynchronous copy in flight and its TMEM released).  A
-// poll also gives up once *err is raised (checked every 32nd poll, so the
-// flag's load does not slow the polling), so one failure ends every slab's
-// level loop at its next missing halo word instead of slab after slab through
-// each one's own timeout.  The failure drill (a.stall) makes one slab
-// publish no halo words, so its neighbours' polls run out.
+// (tma::kSpinLimit polls); a wait that gives up raises *err and the CTA
+// leaves the level loop (with no asynchronous copy in flight and its TMEM
+// released), after which its neighbours' waits run out the same way.
+//
+// Failure drill: a second instantiation (DRILL, generic column pitch) takes
+// the wait limit from a.spin, gives a poll up as soon as *err is raised
+// (checked every 32nd poll) and lets slab a.stall publish its halo words into
+// a spare area that nobody reads, so its neighbours' polls run out.  Only
+// contexts given the test keys launch it: the production instantiations keep
+// the constant limit, whose code the level loop's schedule was tuned with.
 #include <cuda_runtime.h>
 
 #include "kargs.h"
@@ -323,7 +326,7 @@ __device__ __forceinline__ void res_item(const FwdResArgs& a, const float* A, fl
 
 // LDS: the stored column pitch ldz + 8 when known at compile time (every
 // shared-memory offset of the stencil becomes an immediate), 0 for any ldz.
-template <int LDS>
+template <int LDS, bool DRILL>
 __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ SrcList src;
@@ -467,7 +470,10 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
     ulonglong2* stage = reinterpret_cast<ulonglong2*>(smem + 2 * (size_t)(a.wmax + 8) * lds);
     // the halo of the next level is fetched during the last two passes
     const int fetch_at = passes >= 2 ? passes - 2 : 0;
-    const bool publish = (int)blockIdx.x != a.stall;
+    // the drill's stalled slab publishes into the spare area after both parity slots
+    const bool stalled = DRILL && (int)blockIdx.x == a.stall;
+    const size_t mstep = stalled ? 1 : (size_t)a.nslab, mbase = stalled ? 2 * (size_t)a.nslab : blockIdx.x;
+    const uint32_t limit = DRILL ? a.spin : tma::kSpinLimit;
     bool done = !fits;
     for (int t = a.t_begin; t < a.t_end && !done; ++t) {
         float* A = smem + oa;  // Q^t (stencil)
@@ -484,7 +490,7 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
                 if (rec_idx[j] >= 0) a.seis[rec_off[j] + (t - a.tlag)] = rec_d[j] * A[rec_idx[j]];
         }
         const int sample = (t + 1 < a.nt) ? t + 1 : -1;
-        ulonglong2* mine = a.xbuf + (slot * a.nslab + blockIdx.x) * 2 * nw;
+        ulonglong2* mine = a.xbuf + (DRILL ? slot * mstep + mbase : slot * a.nslab + blockIdx.x) * 2 * nw;
         const ulonglong2* from_left = a.xbuf + (slot * a.nslab + (sl.left >= 0 ? sl.left : 0)) * 2 * nw + nw;
         const ulonglong2* from_right = a.xbuf + (slot * a.nslab + (sl.right >= 0 ? sl.right : 0)) * 2 * nw;
         for (int k = 0; k <= passes; ++k) {
@@ -499,8 +505,8 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
             const int pos = s_pos[k * kRC + tid];
             const bool valid = pos >= 0;
             const int c0 = (pos >> 16) & 0x3fff, gz = pos & 0xffff;
-            ulonglong2* pa = (publish && sl.left >= 0 && c0 == 0) ? mine : nullptr;  // the edge runs
-            ulonglong2* pb = (publish && sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
+            ulonglong2* pa = (sl.left >= 0 && c0 == 0) ? mine : nullptr;  // the edge runs
+            ulonglong2* pb = (sl.right >= 0 && c0 + 4 >= sl.w) ? mine + nw : nullptr;
             res_item(a, A, B, lds, c0, gz, valid, (pos & 0x40000000) != 0, tbase + kItemCols * k, src, sample, pa, pb,
                      tag);
         }
@@ -514,19 +520,19 @@ __global__ void __launch_bounds__(kRT, 1) fwd_res_kernel(const FwdResArgs a) {
                 const int w = tid + i * kRT;
                 if (xdst[i] < 0) continue;
                 ulonglong2 v = stage[w];
-                if (ok && !word_is(v, tag)) {
-                    // after one failure the rest of the halo is not awaited
+                if (!word_is(v, tag)) {
                     const ulonglong2* g = w < nw ? from_left + w : from_right + (w - nw);
-                    ok = false;
-                    for (uint32_t spin = 0; spin < a.spin; ++spin) {
+                    uint32_t spin = 0;
+                    for (; spin < limit; ++spin) {
                         v = ld_word(g);
-                        if (word_is(v, tag)) {
-                            ok = true;
+                        if (word_is(v, tag)) break;
+                        if (DRILL && (spin & 31u) == 31u && tma::ld_flag(a.err)) {
+                            spin = limit;  // another slab has failed: give up now
                             break;
                         }
-                        if ((spin & 31u) == 31u && tma::ld_flag(a.err)) break;  // every 32nd poll only
                         __nanosleep(64);
                     }
+                    ok = ok && spin < limit;
                 }
                 *reinterpret_cast<float2*>(B + xdst[i]) =
                     make_float2(__uint_as_float((unsigned)v.x), __uint_as_float((unsigned)v.y));
@@ -573,17 +579,22 @@ constexpr size_t kMinSmem = 116 * 1024;
 // column pitches (ldz + 8) compiled as constants: ldz a multiple of 32 up to 384
 #define FWI_FWD_RES_LDS(X) X(40) X(72) X(104) X(136) X(168) X(200) X(232) X(264) X(296) X(328) X(360) X(392)
 
-const void* res_kernel(int ldz) {
-#define FWI_X(l) if (ldz + 8 == l) return (const void*)fwd_res_kernel<l>;
+const void* res_kernel(int ldz, bool drill) {
+    if (drill) return (const void*)fwd_res_kernel<0, true>;
+#define FWI_X(l) if (ldz + 8 == l) return (const void*)fwd_res_kernel<l, false>;
     FWI_FWD_RES_LDS(FWI_X)
 #undef FWI_X
-    return (const void*)fwd_res_kernel<0>;
+    return (const void*)fwd_res_kernel<0, false>;
 }
+
+bool is_drill(const FwdResArgs& a) { return a.stall >= 0 || a.spin != tma::kSpinLimit; }
 
 cudaError_t res_configure(int ldz, size_t smem, int* ctas) {
     smem = smem < kMinSmem ? kMinSmem : smem;
-    const void* fn = res_kernel(ldz);
+    const void* fn = res_kernel(ldz, false);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(res_kernel(ldz, true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, kRT, smem);
     return e;
 }
@@ -591,7 +602,7 @@ cudaError_t res_configure(int ldz, size_t smem, int* ctas) {
 cudaError_t res_launch(const FwdResArgs& a, size_t smem, cudaStream_t st) {
     smem = smem < kMinSmem ? kMinSmem : smem;
     void* args[] = {const_cast<FwdResArgs*>(&a)};
-    return cudaLaunchCooperativeKernel(res_kernel(a.ldz), dim3(a.nslab), dim3(kRT), args, smem, st);
+    return cudaLaunchCooperativeKernel(res_kernel(a.ldz, is_drill(a)), dim3(a.nslab), dim3(kRT), args, smem, st);
 }
 
 }  // namespace
@@ -614,7 +625,7 @@ size_t fwd_res_smem(int wmax, int ldz) {
 
 size_t fwd_res_static_smem() {
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, fwd_res_kernel<0>) != cudaSuccess) {
+    if (cudaFuncGetAttributes(&fa, fwd_res_kernel<0, false>) != cudaSuccess) {
         cudaGetLastError();
         return sizeof(SrcList) + 64;
     }
