@@ -20,11 +20,13 @@
 //     TX/8 columns, register-window Laplacians) and store the four outputs
 //     with coalesced float4 stores, then release the stage.
 //
-// Every wait is bounded (a.spin polls; a grid-barrier poll also gives up as
-// soon as another CTA has raised *err); a wait that gives up raises *err and
-// the kernel returns once its own copies in flight have landed.  The failure
-// drill (a.stall) makes one CTA withhold the loads of its first tile, so its
-// consumers' and then every other CTA's waits run out.
+// Every wait is bounded (tma::kSpinLimit polls); a wait that gives up raises
+// *err and the kernel returns once its own copies in flight have landed.
+// Failure drill: the DRILL instantiations take the limit from a.spin, give a
+// grid-barrier poll up once *err is raised, and let CTA a.stall withhold the
+// loads of its first tile, so its consumers' and then every other CTA's waits
+// run out.  Only contexts given the test keys launch them; the production
+// instantiations keep the constant limit.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -52,23 +54,16 @@ struct BGeom {
     static constexpr uint32_t BYTES = STAGE * 4;
     static_assert((ST * 4) % 128 == 0 && (PT * 4) % 128 == 0, "TMA destinations must stay 128-byte aligned");
     static_assert(CZ <= 256 && CX <= 256, "TMA box extent");
-    static_assert(TX <= 16, "per-column receiver metadata holds 16 columns");
 };
 
-// Stage metadata, written by the producer warp before the stage's second
-// arrival.  For a tile with receivers (has_rec) the producer's lanes also
-// fetch, per tile column, the row of its receiver in the tile (-1: none) and
-// the injected amplitude of this level; multi: a column holds more than one
-// receiver, the consumers then walk the column table themselves.
 struct BMeta {
-    int s, x0, z0, nxx, col_off, has_rec, multi;
-    int zrow[16];
-    float amp[16];
+    int s, x0, z0, nxx, col_off, has_rec;
 };
 
-// Gives up after `limit` polls, or when another CTA has raised *err (that CTA
-// has left the level loop and will never arrive; checked every 32nd poll so
-// that the flag's load does not slow the barrier).
+// Gives up after `limit` polls; the drill instantiation also gives up when
+// another CTA has raised *err (that CTA has left the level loop and will
+// never arrive; checked every 32nd poll).
+template <bool DRILL>
 __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, uint32_t limit, const int* err) {
     __threadfence();
     atomicAdd(counter, 1u);
@@ -76,7 +71,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
         if (v >= target) return true;
-        if ((i & 31u) == 31u && tma::ld_flag(err)) return false;  // every 32nd poll only
+        if (DRILL && (i & 31u) == 31u && tma::ld_flag(err)) return false;
         __nanosleep(64);
     }
     return false;
@@ -121,6 +116,15 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
     const float* t_b = t_v + 4 * G::PT;
     const st::Rows rows = st::rows_info(nullptr, 0, z, a.nzz);
     const int c0 = warp * CPW;
+    // the receivers of the thread's columns, fetched before the stencil so
+    // that the load's latency hides behind the shared-memory work
+    int4 rc[CPW];
+#pragma unroll
+    for (int m = 0; m < CPW; ++m) {
+        rc[m] = make_int4(0, 0, 0, 0);
+        if (mt.has_rec && mt.x0 + c0 + m < mt.nxx)
+            rc[m] = __ldg(reinterpret_cast<const int4*>(a.rec_col + mt.col_off + mt.x0 + c0 + m));
+    }
     float ls[CPW][4], lr[CPW][4];
     float4 psold[CPW], pr[CPW];
     st::lap_run<G::CZ, CPW>(t_ps, 4 * lane + 4, c0 + 4, ls, psold);
@@ -142,16 +146,18 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
                                                        a.dt2idh2, a.dt, a.idh2, rows, colok);
         float4 rv = r.pr;
         if (mt.has_rec) {
-            if (mt.multi) {
-                st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
-            } else {
-                // the producer fetched this column's receiver row and amplitude
-                const int dz = mt.zrow[c] - z;
-                const float amp = mt.amp[c];
+            // rc = {row, count, trace offset}: one receiver in the column is
+            // added here; columns with more take the column-table walk
+            const int dz = rc[m].x - z;
+            if (rc[m].y == 1 && dz >= 0 && dz < 4) {
+                const long long soff = ((long long)(unsigned)rc[m].w << 32) | (unsigned)rc[m].z;
+                const float amp = a.inj.scale * __ldg(a.inj.series + soff + sample);
                 if (dz == 0) rv.x += amp;
                 else if (dz == 1) rv.y += amp;
                 else if (dz == 2) rv.z += amp;
-                else if (dz == 3) rv.w += amp;
+                else rv.w += amp;
+            } else if (rc[m].y > 1) {
+                st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
             }
         }
         const size_t g = so + (size_t)gx * a.ldz + z;
@@ -162,7 +168,7 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
     }
 }
 
-template <int TX, int S, bool GRAD>
+template <int TX, int S, bool GRAD, bool DRILL>
 __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
     bwd_loop_kernel(const __grid_constant__ BwdLoopMaps maps, const BwdLoopArgs a) {
     using G = BGeom<TX>;
@@ -177,7 +183,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
 
     if (tid == 0) {
         for (int k = 0; k < S; ++k) {
-            tma::mbar_init(&full[k], 2);  // the loads' transaction bytes + the metadata arrival
+            tma::mbar_init(&full[k], 1);
             tma::mbar_init(&empty[k], kNC / 32);
         }
         abort_flag = 0;
@@ -188,6 +194,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
     }
     __syncthreads();
 
+    const uint32_t limit = DRILL ? a.spin : tma::kSpinLimit;
     int issued = 0;  // producer lane: loads issued so far
     int k = 0;       // pipeline use counter, continuous across levels
     for (int b = a.b_begin; b < a.b_end; ++b) {
@@ -195,36 +202,29 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
         const int sample = (b + 1 < a.nt) ? a.nt - 1 - (b + 1) : -1;
         bool ok = true;
         if (tid >= kNC) {
-            // ---------- producer warp: lane 0 streams this level's tiles with
-            // TMA; for tiles with receivers all lanes then fetch the level's
-            // amplitudes into the stage metadata, and lane 0 adds the stage's
-            // second arrival once they are written
-            if (lane == 0) fence_proxy_async_global();
-            int kk = k;
-            for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
-                const int stg = kk % S;
-                bool free_stage = true;
-                if (lane == 0 && kk >= S)
-                    free_stage = tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), a.spin);
-                if (!__shfl_sync(0xffffffffu, free_stage, 0)) {
-                    ok = false;
-                    break;
-                }
-                if (a.stall == (int)blockIdx.x && b == a.b_begin && kk == k) continue;  // failure drill
-                const ft::TileInfo ti = decode_tile(a, tile, TX);
-                const int s = ti.s, z0 = ti.z0, x0 = ti.x0;
-                const ShotDesc sd = a.shots[s];
-                BMeta& mt = meta[stg];
-                // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
-                const bool rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
-                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
-                if (lane == 0) {
+            // ---------- producer: lane 0 streams this level's tiles
+            if (lane == 0) {
+                fence_proxy_async_global();
+                int kk = k;
+                for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
+                    const int stg = kk % S;
+                    if (kk >= S && !tma::mbar_wait(&empty[stg], (uint32_t)(((kk / S) - 1) & 1), limit)) {
+                        ok = false;
+                        break;
+                    }
+                    if (DRILL && a.stall == (int)blockIdx.x && b == a.b_begin && kk == k) continue;  // the drill
+                    const ft::TileInfo ti = decode_tile(a, tile, TX);
+                    const int s = ti.s, z0 = ti.z0, x0 = ti.x0;
+                    const ShotDesc sd = a.shots[s];
+                    BMeta& mt = meta[stg];
                     mt.s = s;
                     mt.x0 = x0;
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    mt.has_rec = rec;
+                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
+                    mt.has_rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
+                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
@@ -235,36 +235,12 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     tma::load_3d(pts + 2 * G::PT, &maps.pr_pt[p], z0, x0, s, &full[stg]);
                     tma::load_3d(pts + 3 * G::PT, &maps.acc_a, z0, x0, s, &full[stg]);
                     tma::load_3d(pts + 4 * G::PT, &maps.acc_b, z0, x0, s, &full[stg]);
-                }
-                if (rec) {
-                    // lane j: column x0 + j; rc = {row, count, trace offset of the first}
-                    int zr = -1, many = 0;
-                    float amp = 0.0f;
-                    if (lane < TX && x0 + lane < sd.nxx) {
-                        const int4 rc = __ldg(reinterpret_cast<const int4*>(a.rec_col + sd.col_off + x0 + lane));
-                        many = rc.y > 1;
-                        if (rc.y == 1 && rc.x >= z0 && rc.x < z0 + kTZ) {
-                            const long long soff = ((long long)(unsigned)rc.w << 32) | (unsigned)rc.z;
-                            zr = rc.x;
-                            amp = a.inj.scale * __ldg(a.inj.series + soff + sample);
-                        }
-                    }
-                    const unsigned multi = __ballot_sync(0xffffffffu, many);
-                    if (lane < TX) {
-                        mt.zrow[lane] = zr;
-                        mt.amp[lane] = amp;
-                    }
-                    if (lane == 0) mt.multi = multi != 0u;
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    tma::mbar_arrive(&full[stg]);  // the metadata is complete
                     issued = kk + 1;
                 }
-            }
-            if (!ok && lane == 0) {
-                atomicExch(a.err, 1);
-                abort_flag = 1;
+                if (!ok) {
+                    atomicExch(a.err, 1);
+                    abort_flag = 1;
+                }
             }
         } else {
             // ---------- consumers
@@ -273,13 +249,13 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
             int kk = k;
             for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++kk) {
                 const int stg = kk % S;
-                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1), a.spin)) {
+                if (!tma::mbar_wait(&full[stg], (uint32_t)((kk / S) & 1), limit)) {
                     if (lane == 0) atomicExch(a.err, 1);
                     abort_flag = 1;
                     ok = false;
                     break;
                 }
-                const BMeta& mt = meta[stg];  // read in place: rewritten only after this stage is released
+                const BMeta mt = meta[stg];
                 const float* stage = smem + stg * G::STAGE;
                 if (st::tile_inner(mt.z0, kTZ, mt.x0, TX, a.nzz, mt.nxx))
                     bwd_tile<TX, GRAD, false>(a, stage, mt, sample, ps_out, pr_out);
@@ -292,7 +268,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
         // the CTA's tiles of level b are written: grid barrier
         __syncthreads();
         if (tid == 0 && !abort_flag) {
-            if (!grid_barrier(a.sync, (unsigned)(b - a.b_begin + 1) * gridDim.x, a.spin, a.err)) {
+            if (!grid_barrier<DRILL>(a.sync, (unsigned)(b - a.b_begin + 1) * gridDim.x, limit, a.err)) {
                 atomicExch(a.err, 1);
                 abort_flag = 1;
             }
@@ -302,7 +278,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
             // never leave copies in flight behind an exiting CTA
             if (tid == kNC)
                 for (int q = (issued > S ? issued - S : 0); q < issued; ++q)
-                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), a.spin);
+                    tma::mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), limit);
             return;
         }
         for (int tile = blockIdx.x; tile < total; tile += gridDim.x) ++k;
@@ -316,9 +292,12 @@ constexpr size_t bwd_smem() {
 
 template <int TX, int S, bool GRAD>
 cudaError_t bwd_configure_one(int* ctas) {
-    auto fn = bwd_loop_kernel<TX, S, GRAD>;
+    auto fn = bwd_loop_kernel<TX, S, GRAD, false>;
     const size_t smem = bwd_smem<TX, S>();
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(bwd_loop_kernel<TX, S, GRAD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, kNT, smem);
 }
@@ -336,11 +315,12 @@ template <int TX, int S>
 cudaError_t bwd_launch(bool gradient, const BwdLoopMaps& maps, const BwdLoopArgs& la, int grid, cudaStream_t st) {
     const size_t smem = bwd_smem<TX, S>();
     void* args[] = {const_cast<BwdLoopMaps*>(&maps), const_cast<BwdLoopArgs*>(&la)};
-    if (gradient)
-        return cudaLaunchCooperativeKernel((const void*)bwd_loop_kernel<TX, S, true>, dim3(grid), dim3(kNT), args,
-                                           smem, st);
-    return cudaLaunchCooperativeKernel((const void*)bwd_loop_kernel<TX, S, false>, dim3(grid), dim3(kNT), args, smem,
-                                       st);
+    const bool drill = la.stall >= 0 || la.spin != tma::kSpinLimit;
+    const void* fn = gradient ? (drill ? (const void*)bwd_loop_kernel<TX, S, true, true>
+                                       : (const void*)bwd_loop_kernel<TX, S, true, false>)
+                              : (drill ? (const void*)bwd_loop_kernel<TX, S, false, true>
+                                       : (const void*)bwd_loop_kernel<TX, S, false, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kNT), args, smem, st);
 }
 
 #define FWI_BWD_LOOP_VARIANTS(X) X(16, 3) X(16, 2) X(8, 4) X(8, 3)
