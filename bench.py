@@ -15,11 +15,19 @@ through libfwi2d's C ABI.  Metric: FD grid-point updates per second
             update (read v, Q^t, Q^{t-1}; write Q^{t+1}) x points per launch,
             over the average launch time in the timed region.
   cpu_baseline  the oracle's float restatement of compute_pressure +
-            compute_seismogram (OpenMP over all host cores) on one shot.
+            compute_seismogram (OpenMP over all host cores) on the survey.
+  batched_survey  RTM of the 240-shot windowed survey: forward and backward
+            kernels' algorithmic GB/s against the HBM peak.
+  rtm_benchmark_geometry  RTM and FWI-gradient kernels on the survey's
+            geometry (100-cell random boundary), updates/s.
+  fwi       FWI of the 81-shot and of the 240-shot windowed surveys: seconds
+            per iteration, misfit and model error per iteration.
 
 --impl reference runs the reference's own CUDA build (oracle/_ref/modeling.exe,
 compiled from the reference sources for sm_100a) on the same survey and reports
-updates / its own "Run time"; without that build it times the CPU port.
+updates / its own "Run time" (without that build it times the CPU port), and
+times the reference's own forward, migration and adjoint loops on the same
+geometry (oracle/_ref/ref_harness --time).
 
 Multi-GPU (torchrun): every rank models its own copy of the survey (shots are
 independent; no data-path collective) -> weak scaling; time = max over ranks.
@@ -196,7 +204,10 @@ def run_reference(args, rank, world):
                                             "sources, FFTW via cuFFTW, sm_100a) on the full 11-shot survey, its "
                                             "'Run time' (shot loop incl. per-shot file writes); runs on the B200"},
                     e2e={"value": value, "unit": "grid-pt updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                    reference_build="oracle/_ref/modeling.exe", slowest_step_s=t)
+                    reference_build="oracle/_ref/modeling.exe", slowest_step_s=t,
+                    note="the reference's 'Run time' covers its shot loop including a terminal clear and one "
+                         "3 MB seismogram file write per shot; the other arm's e2e includes the host copies "
+                         "but no file writes")
         if not args.no_batched:
             back = reference_backward(case, vp)
             if back:
@@ -552,6 +563,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 4-layer + anomaly model, 151x501 at 10 m)",
         "config": {"workload": WORKLOAD, "shots_per_rank": d.nsrc, "grid": [d.nzz, d.nxx], "time_steps": n_steps,
+                   "boundary": "100-cell absorbing boundary (ABC), as the reference's modeling.exe models",
                    "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"shot replicas x{world}"},
         "e2e": {"value": world * ups / (e2e_ms * 1e-3), "unit": "grid-pt updates/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(h_model.numel() * 4), "d2h_bytes_per_step": int(nseis * 4)},
