@@ -1353,7 +1353,6 @@ void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Table
     a.pr[1] = pr[1];
     a.acc_a = acc_[0];
     a.acc_b = acc_[1];
-    a.rec_col = t.d_rec_col;
     a.err = d_err_;
     a.sync = d_sync_;
     a.spin = spin_limit_;

@@ -26,7 +26,8 @@
 // grid-barrier poll up once *err is raised, and let CTA a.stall withhold the
 // loads of its first tile, so its consumers' and then every other CTA's waits
 // run out.  Only contexts given the test keys launch them; the production
-// instantiations keep the constant limit.
+// instantiations keep the constant limit (whose code the kernel was measured
+// with: even a run-time limit changes the schedule).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -116,15 +117,6 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
     const float* t_b = t_v + 4 * G::PT;
     const st::Rows rows = st::rows_info(nullptr, 0, z, a.nzz);
     const int c0 = warp * CPW;
-    // the receivers of the thread's columns, fetched before the stencil so
-    // that the load's latency hides behind the shared-memory work
-    int4 rc[CPW];
-#pragma unroll
-    for (int m = 0; m < CPW; ++m) {
-        rc[m] = make_int4(0, 0, 0, 0);
-        if (mt.has_rec && mt.x0 + c0 + m < mt.nxx)
-            rc[m] = __ldg(reinterpret_cast<const int4*>(a.rec_col + mt.col_off + mt.x0 + c0 + m));
-    }
     float ls[CPW][4], lr[CPW][4];
     float4 psold[CPW], pr[CPW];
     st::lap_run<G::CZ, CPW>(t_ps, 4 * lane + 4, c0 + 4, ls, psold);
@@ -145,21 +137,7 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
         const st::Bwd4 r = st::bwd_update4<GRAD, EDGE>(ls[m], psold[m], lr[m], pr[m], ps, prold, vv, ga, gb,
                                                        a.dt2idh2, a.dt, a.idh2, rows, colok);
         float4 rv = r.pr;
-        if (mt.has_rec) {
-            // rc = {row, count, trace offset}: one receiver in the column is
-            // added here; columns with more take the column-table walk
-            const int dz = rc[m].x - z;
-            if (rc[m].y == 1 && dz >= 0 && dz < 4) {
-                const long long soff = ((long long)(unsigned)rc[m].w << 32) | (unsigned)rc[m].z;
-                const float amp = a.inj.scale * __ldg(a.inj.series + soff + sample);
-                if (dz == 0) rv.x += amp;
-                else if (dz == 1) rv.y += amp;
-                else if (dz == 2) rv.z += amp;
-                else rv.w += amp;
-            } else if (rc[m].y > 1) {
-                st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
-            }
-        }
+        if (mt.has_rec) st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
         const size_t g = so + (size_t)gx * a.ldz + z;
         *reinterpret_cast<float4*>(ps_out + g) = r.ps;
         *reinterpret_cast<float4*>(pr_out + g) = rv;
@@ -222,9 +200,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
-                    mt.has_rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
-                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
+                    mt.has_rec = sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);

@@ -33,7 +33,8 @@ struct ShotDesc {
 
 // Receivers of one grid column of a shot (entry col_off + x, as the receiver
 // column table): how many, and the row and trace offset of the first.  The
-// back-propagation kernel reads it instead of walking the column table.
+// multi-level forward kernel records from it instead of walking the column
+// table.
 struct __align__(16) RecCol {
     int z;
     int n;
@@ -166,7 +167,6 @@ struct BwdLoopArgs {
     float* pr[2];
     float* acc_a;
     float* acc_b;
-    const RecCol* rec_col;    // per-column receivers (indexed like inj.colptr)
     int* err;
     unsigned* sync;           // grid-barrier counter, zero at launch
     unsigned spin;            // polls of a bounded wait before it gives up
