@@ -21,8 +21,6 @@
 //     float32 NHWC rows.
 // Every mbarrier wait is bounded; a wait that gives up raises g_tc_err
 // (fwi_nn_check) and the CTA still waits (bounded) before freeing its TMEM.
-#include <algorithm>
-
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -36,7 +34,6 @@ namespace {
 
 constexpr int kTcM = 128;        // pixels per CTA tile = TMEM lanes
 constexpr int kTcThreads = 128;  // 4 warps; warp w reads TMEM lanes 32w..32w+31
-constexpr int kTcMaxStages = 4;  // shared-memory stages of the copy / MMA pipeline
 
 __device__ int g_tc_err;
 
@@ -89,15 +86,10 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t 
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(dst)), "l"(src), "r"(src_bytes)
                  : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Wait until at most `pending` of the thread's cp.async groups are still in
-// flight (0..3), then make the landed copies visible to the tensor cores'
-// (async proxy) reads.
-__device__ __forceinline__ void cp_async_wait_async_proxy(int pending) {
-    if (pending <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
-    else if (pending == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
-    else if (pending == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
-    else asm volatile("cp.async.wait_group 3;" ::: "memory");
+// Wait for every cp.async of the thread, then make the copies visible to the
+// tensor cores' (async proxy) reads.
+__device__ __forceinline__ void cp_async_wait_all_async_proxy() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
@@ -109,11 +101,11 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ in, int N, int H,
                                                                 int W, int Cin, const __nv_bfloat16* __restrict__ w,
                                                                 const float* __restrict__ bias, int Cout, int ncols,
-                                                                uint32_t stage_bytes, int nst, int relu,
+                                                                uint32_t stage_bytes, int relu,
                                                                 __nv_bfloat16* __restrict__ out,
                                                                 float* __restrict__ out32) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar[kTcMaxStages];
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
     const long long P = (long long)N * H * W;
@@ -128,7 +120,8 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
         tc_fence_before();
     }
     if (tid == 0) {
-        for (int k = 0; k < nst; ++k) tma::mbar_init(&bar[k], 1);
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
@@ -143,10 +136,14 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
         y = (int)(r % H);
         n = (int)(r / H);
     }
-    // copies of tap t into stage t % nst, as one cp.async group of the thread
-    auto stage_tap = [=](int tap) {
-        unsigned char* A = smem + (size_t)(tap % nst) * stage_bytes;
+    const uint32_t idesc = umma_idesc(kTcM, Cout);
+    bool ok = true;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int s = tap & 1;
+        unsigned char* A = smem + (size_t)s * stage_bytes;
         unsigned char* B = A + a_bytes;
+        // the stage's previous MMAs (tap - 2) must be done before it is rewritten
+        if (tap >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((tap - 2) >> 1) & 1))) ok = false;
         const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
         const bool in_ok = valid && yy >= 0 && yy < H && xx >= 0 && xx < W;
         const uint4* src = reinterpret_cast<const uint4*>(in + (((long long)n * H + (in_ok ? yy : 0)) * W +
@@ -159,39 +156,21 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
             cp_async16(B + ((size_t)(co >> 3) * kc + j) * 128 + (co & 7) * 16,
                        reinterpret_cast<const uint4*>(w + ((long long)co * 9 + tap) * Cin) + j, 16u);
         }
-        cp_async_commit();
-    };
-    const uint32_t idesc = umma_idesc(kTcM, Cout);
-    bool ok = true;
-    // software pipeline: the copies of tap t + nst - 1 are issued while those
-    // of taps t .. t + nst - 2 are in flight and the MMAs of tap t - 1 run
-    for (int t = 0; t < nst - 1; ++t) stage_tap(t);
-    for (int tap = 0; tap < 9; ++tap) {
-        const int nxt = tap + nst - 1;
-        if (nxt < 9) {
-            // stage nxt % nst last held tap nxt - nst = tap - 1: its MMAs must be done
-            if (nxt >= nst && !tma::mbar_wait(&bar[nxt % nst], (uint32_t)(((nxt - nst) / nst) & 1))) ok = false;
-            stage_tap(nxt);
-        } else {
-            cp_async_commit();  // an empty group keeps the count of groups per iteration fixed
-        }
-        cp_async_wait_async_proxy(nst - 1);  // tap's copies have landed
+        cp_async_wait_all_async_proxy();  // the tensor cores read these copies through the async proxy
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t sa = saddr(smem + (size_t)(tap % nst) * stage_bytes), sb = sa + a_bytes;
+            const uint32_t sa = saddr(A), sb = saddr(B);
             for (int k = 0; k < Cin / 16; ++k)
                 umma_bf16(tmem, umma_desc(sa + 256u * k, 128u, (uint32_t)kc * 128u),
                           umma_desc(sb + 256u * k, 128u, (uint32_t)kc * 128u), idesc, (tap | k) != 0 ? 1u : 0u);
-            umma_commit(&bar[tap % nst]);
+            umma_commit(&bar[s]);
         }
     }
-    // the last use of every stage is collected, so no arrival lands after exit
-    // (tap 8's commit also covers every earlier MMA of the CTA)
-    for (int st = 0; st < nst; ++st) {
-        const int last = st + ((8 - st) / nst) * nst;  // the last tap on stage st
-        if (!tma::mbar_wait(&bar[st], (uint32_t)((last / nst) & 1))) ok = false;
-    }
+    // tap 8 (stage 0, its 5th use) commits after every earlier MMA; the last
+    // arrival on stage 1 (tap 7) is collected too, so none lands after exit
+    if (!tma::mbar_wait(&bar[0], 0u)) ok = false;
+    if (!tma::mbar_wait(&bar[1], 1u)) ok = false;
     tc_fence_after();
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
     for (int c0 = 0; c0 < Cout; c0 += 8) {
@@ -241,10 +220,9 @@ constexpr int kWgK = 64;  // pixels per stage
 __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ in,
                                                               const __nv_bfloat16* __restrict__ dout, int N, int H,
                                                               int W, int Cin, int Cout, int chunk, int ncols,
-                                                              uint32_t stage_bytes, int nst,
-                                                              float* __restrict__ partial) {
+                                                              uint32_t stage_bytes, float* __restrict__ partial) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar[kTcMaxStages];
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int tap = blockIdx.y;
@@ -262,7 +240,8 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
         tc_fence_before();
     }
     if (tid == 0) {
-        for (int k = 0; k < nst; ++k) tma::mbar_init(&bar[k], 1);
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
@@ -271,10 +250,12 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
     // M = 128, N = Cin, both operands MN-major (bits 15 and 16)
     const uint32_t idesc = umma_idesc(128, Cin) | (1u << 15) | (1u << 16);
     const int nstage = p_end > p_begin ? (int)((p_end - p_begin + kWgK - 1) / kWgK) : 0;
-    // copies of pixel stage st into shared-memory stage st % nst, one cp.async group
-    auto stage_pixels = [=](int st) {
-        unsigned char* A = smem + (size_t)(st % nst) * stage_bytes;
+    bool ok = true;
+    for (int st = 0; st < nstage; ++st) {
+        const int s = st & 1;
+        unsigned char* A = smem + (size_t)s * stage_bytes;
         unsigned char* B = A + a_bytes;
+        if (st >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((st - 2) >> 1) & 1))) ok = false;
         const long long q0 = p_begin + (long long)st * kWgK;
         // A: dout rows (pixels) x co, 16 co groups x 64 pixels (zeros past the
         // chunk and past Cout; the copy's source is then pixel p_begin, channel 0)
@@ -300,35 +281,21 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
                        reinterpret_cast<const uint4*>(in + (ok_b ? (q + (long long)dy * W + dx) * Cin + ni * 8 : 0)),
                        ok_b ? 16u : 0u);
         }
-        cp_async_commit();
-    };
-    bool ok = true;
-    // software pipeline over the pixel stages, as the convolution's taps
-    for (int st = 0; st < nst - 1 && st < nstage; ++st) stage_pixels(st);
-    for (int st = 0; st < nstage; ++st) {
-        const int nxt = st + nst - 1;
-        if (nxt < nstage) {
-            // shared-memory stage nxt % nst last held pixel stage st - 1: its MMAs must be done
-            if (nxt >= nst && !tma::mbar_wait(&bar[nxt % nst], (uint32_t)(((nxt - nst) / nst) & 1))) ok = false;
-            stage_pixels(nxt);
-        } else {
-            cp_async_commit();  // an empty group keeps the count of groups per iteration fixed
-        }
-        cp_async_wait_async_proxy(nst - 1);  // stage st's copies have landed
+        cp_async_wait_all_async_proxy();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t sa = saddr(smem + (size_t)(st % nst) * stage_bytes), sb = sa + a_bytes;
+            const uint32_t sa = saddr(A), sb = saddr(B);
             for (int k = 0; k < kWgK / 16; ++k)
                 umma_bf16(tmem, umma_desc(sa + 256u * k, 128u, 1024u), umma_desc(sb + 256u * k, 128u, 1024u), idesc,
                           (st | k) != 0 ? 1u : 0u);
-            umma_commit(&bar[st % nst]);
+            umma_commit(&bar[s]);
         }
     }
-    // collect the last use of every shared-memory stage
-    for (int s = 0; s < nst && s < nstage; ++s) {
-        const int last = s + ((nstage - 1 - s) / nst) * nst;  // the last pixel stage on it
-        if (!tma::mbar_wait(&bar[s], (uint32_t)((last / nst) & 1))) ok = false;
+    // collect the last use of each stage
+    for (int s = 0; s < 2; ++s) {
+        const int last = nstage - 1 - ((nstage - 1 - s) & 1);  // last stage index with parity s
+        if (last >= 0 && last % 2 == s && !tma::mbar_wait(&bar[s], (uint32_t)((last >> 1) & 1))) ok = false;
     }
     tc_fence_after();
     const int co = tid;  // TMEM lane = output channel
@@ -362,20 +329,14 @@ int nn_wgrad_tc(const void* in, const void* dout, int N, int H, int W, int Cin, 
     int ncols = 32;
     while (ncols < Cin) ncols *= 2;
     const uint32_t stage = 16u * 8u * 128u + (uint32_t)Cin * 128u;
-    // as many pipeline stages (2..4) as fit next to the static shared memory
-    static size_t static_smem = 0;
-    if (!static_smem) {
-        cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, wgrad_tc_kernel) != cudaSuccess) return -2;
-        static_smem = fa.sharedSizeBytes;
-    }
-    const int nst = (int)std::min<size_t>(kTcMaxStages, (227 * 1024 - static_smem) / stage);
-    if (nst < 2) return -1;
-    size_t smem = (size_t)nst * stage;
+    size_t smem = 2 * (size_t)stage;
     const size_t tmem_share = (size_t)ncols * 460;
     if (smem < tmem_share) smem = tmem_share;
     static size_t configured = 0;
     if (smem > configured) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, wgrad_tc_kernel) != cudaSuccess) return -2;
+        if (smem + fa.sharedSizeBytes > 227 * 1024) return -1;
         if (cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return -2;
@@ -383,7 +344,7 @@ int nn_wgrad_tc(const void* in, const void* dout, int N, int H, int W, int Cin, 
     }
     wgrad_tc_kernel<<<dim3(chunks, 9), kTcThreads, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
                                                                static_cast<const __nv_bfloat16*>(dout), N, H, W, Cin,
-                                                               Cout, chunk, ncols, stage, nst, partial);
+                                                               Cout, chunk, ncols, stage, partial);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -393,24 +354,18 @@ int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, c
     int ncols = 32;
     while (ncols < Cout) ncols *= 2;
     const uint32_t stage = ((uint32_t)(kTcM * Cin + Cout * Cin) * 2u + 1023u) / 1024u * 1024u;
-    // as many pipeline stages (2..4) as fit next to the static shared memory
-    static size_t static_smem = 0;
-    if (!static_smem) {
-        cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, conv3x3_tc_kernel) != cudaSuccess) return -2;
-        static_smem = fa.sharedSizeBytes;
-    }
-    const size_t avail = 227 * 1024 - static_smem;
-    const int nst = (int)std::min<size_t>(kTcMaxStages, avail / stage);
-    if (nst < 2) return -1;  // two stages do not fit: unsupported size
     // at most 512 TMEM columns of resident CTAs per SM: ask for enough shared
     // memory that no more CTAs than that fit
-    size_t smem = (size_t)nst * stage;
+    size_t smem = 2 * (size_t)stage;
     const size_t tmem_share = (size_t)ncols * 460;
     if (smem < tmem_share) smem = tmem_share;
-    // dynamic shared memory above the default needs the attribute
+    // dynamic shared memory above the default needs the attribute (the
+    // static 1 KB of barriers and alignment comes on top of it)
     static size_t configured = 0;
     if (smem > configured) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, conv3x3_tc_kernel) != cudaSuccess) return -2;
+        if (smem + fa.sharedSizeBytes > 227 * 1024) return -1;  // two stages do not fit: unsupported size
         if (cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return -2;
@@ -420,7 +375,7 @@ int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, c
     const unsigned grid = (unsigned)((P + kTcM - 1) / kTcM);
     conv3x3_tc_kernel<<<grid, kTcThreads, smem, st>>>(
         static_cast<const __nv_bfloat16*>(in), N, H, W, Cin, static_cast<const __nv_bfloat16*>(w), bias, Cout, ncols,
-        stage, nst, relu, static_cast<__nv_bfloat16*>(out), out32);
+        stage, relu, static_cast<__nv_bfloat16*>(out), out32);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
