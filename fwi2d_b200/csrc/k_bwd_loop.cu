@@ -200,7 +200,9 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    mt.has_rec = sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
+                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
+                    mt.has_rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
+                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);

@@ -129,3 +129,41 @@ def test_benchmark_geometry_rtm_section_vs_oracle(rtm):
           f"engine's raw image {e_own:.3e}")
     assert e_own < 1e-6
     assert e_ref < RTOL
+
+
+def test_benchmark_geometry_gradient_vs_oracle(survey, tmp_path):
+    """FWI gradient of the benchmark geometry (inversion.cu:111-166, 213-248,
+    381-444): misfit of the smoothed model against the survey's data, raw
+    gradient and illumination through the random boundary of every shot,
+    against the FP64 oracle run on the engine's own boundary velocities."""
+    c, vp = synth.modeling_survey(tmp_path, seed=0)
+    smooth = synth.smooth_model(vp, c.dh, 150.0)
+    obs = survey["refs"][64].astype(np.float32)
+    with api.Context(c.params, api.MODE_INVERSION) as ctx:
+        ctx.set_model(smooth)
+        ctx.set_observed(obs)
+        vels = [ctx.random_boundary(s) for s in range(len(c.sx))]
+        sum_res = ctx.compute_gradient(True)
+        graw, gill = ctx.gradient_raw()
+        plan = ctx.describe()
+    wav, tlag = survey["wav"], survey["tlag"]
+    vel_abc, tab = O.expand(smooth, NB), O.b1d(NB, 0.004)
+    ref_sum = 0.0
+    acc = np.zeros(vels[0].shape, np.float64)
+    ill = np.zeros_like(acc)
+    for s in range(len(c.sx)):
+        src = (survey["sx"][s], survey["sz"][s])
+        cal = O.forward(vel_abc, NB, tab, wav, c.nt, tlag, c.dt, c.dh, src, survey["rx"], survey["rz"], bits=64)[0]
+        res = obs[s].astype(np.float64) - cal
+        ref_sum += float((res * res).sum())
+        _, P, Po = O.forward(vels[s], NB, None, wav, c.nt, tlag, c.dt, c.dh, src, survey["rx"], survey["rz"], bits=64)
+        a, b = O.backward(vels[s], res.astype(np.float32), c.nt, tlag, c.dt, c.dh, survey["rx"], survey["rz"], P, Po,
+                          gradient=True, bits=64)
+        acc += a
+        ill += b
+    e_sum = abs(sum_res - ref_sum) / ref_sum
+    e_g = rel_l2(graw, O.crop(acc, NB))
+    e_i = rel_l2(gill, O.crop(ill, NB))
+    print(f"\n[full-length gradient] misfit {e_sum:.3e}, raw gradient {e_g:.3e}, illumination {e_i:.3e} "
+          f"vs FP64 oracle ({plan.split('|')[0].strip()})")
+    assert e_sum < RTOL and e_g < RTOL and e_i < RTOL
