@@ -200,9 +200,7 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
-                    mt.has_rec = sample >= 0 && z0 <= sd.rec_zmax && z0 + kTZ > sd.rec_zmin &&
-                                 st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
+                    mt.has_rec = sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);

@@ -107,7 +107,6 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
-    __shared__ long long s_src[kTcM];  // per tap: element offset of each pixel's input row, -1: zeros
     const int tid = threadIdx.x, warp = tid >> 5;
     const long long P = (long long)N * H * W;
     const long long p = (long long)blockIdx.x * kTcM + tid;  // this thread's pixel (A row, TMEM lane)
@@ -147,28 +146,11 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
         if (tap >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((tap - 2) >> 1) & 1))) ok = false;
         const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
         const bool in_ok = valid && yy >= 0 && yy < H && xx >= 0 && xx < W;
-        s_src[tid] = in_ok ? (((long long)n * H + yy) * W + xx) * Cin : -1;
-        __syncthreads();
-        // A_tap: copy e = tid + 128 i takes pixel pg * 8 + (e & 7), channels
-        // 8 j .. 8 j + 7 (rest = e >> 3 = pg * kc + j): eight consecutive
-        // threads fill one 128-byte row of core matrices, and a warp reads
-        // four 16-byte chunks of each of eight pixels
-        {
-            const int p8 = tid & 7;
-            int j = (tid >> 3) % kc, pg = (tid >> 3) / kc;
-            const int q16 = 16 / kc, r16 = 16 % kc;  // rest advances by 16 per copy
-            for (int i = 0; i < kc; ++i) {
-                const long long off = s_src[pg * 8 + p8];
-                cp_async16(A + ((size_t)pg * kc + j) * 128 + p8 * 16,
-                           reinterpret_cast<const uint4*>(in + (off >= 0 ? off : 0)) + j, off >= 0 ? 16u : 0u);
-                j += r16;
-                pg += q16;
-                if (j >= kc) {
-                    j -= kc;
-                    ++pg;
-                }
-            }
-        }
+        const uint4* src = reinterpret_cast<const uint4*>(in + (((long long)n * H + (in_ok ? yy : 0)) * W +
+                                                                (in_ok ? xx : 0)) * Cin);
+        unsigned char* arow = A + (size_t)(tid >> 3) * kc * 128 + (tid & 7) * 16;
+        const uint32_t a_src = in_ok ? 16u : 0u;
+        for (int j = 0; j < kc; ++j) cp_async16(arow + (size_t)j * 128, src + j, a_src);
         for (int e = tid; e < Cout * kc; e += kTcThreads) {
             const int co = e / kc, j = e - co * kc;
             cp_async16(B + ((size_t)(co >> 3) * kc + j) * 128 + (co & 7) * 16,
