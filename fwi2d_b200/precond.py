@@ -111,9 +111,12 @@ TRAIN_SEED0 = 1000  # training models use seeds TRAIN_SEED0 ..; test models use 
 
 
 def make_pairs(root, models: int, stages: int = 4, seed0: int = TRAIN_SEED0, setup: PairSetup = PairSetup(),
-               log=print):
+               log=print, net: cnn.UNet | None = None):
     """models x stages pairs -> (X: [n, P*16] bf16, T: [n, P] float32) on the device.
-    Stage k of a model is its k-th plain-FWI iterate from the 1-D start."""
+    Stage k of a model is its k-th FWI iterate from the 1-D start: plain FWI,
+    or, given a network, the network-preconditioned iteration of fwi() (pairs
+    along the trajectories the preconditioner itself takes, whose models are
+    much closer to the truth than plain FWI's after the first step)."""
     torch = _torch()
     root = Path(root)
     s = setup
@@ -144,11 +147,32 @@ def make_pairs(root, models: int, stages: int = 4, seed0: int = TRAIN_SEED0, set
                 k += 1
                 if st + 1 < stages:
                     ctx.gradient_finish()
-                    step, _, _ = line_search(ctx, float(np.sqrt(np.float32(sum_res))))
+                    f0 = float(np.sqrt(np.float32(sum_res)))
+                    if net is not None:
+                        _network_direction(ctx, net, X[k - 1])
+                        step, f1, f2 = line_search(ctx, f0)
+                        if step <= 0.0 or min(f1, f2) >= f0:
+                            ctx.gradient_finish()  # back to the illumination-normalised gradient
+                            step, _, _ = line_search(ctx, f0)
+                    else:
+                        step, _, _ = line_search(ctx, f0)
                     ctx.update_model_bounded(step, VMIN, VMAX)
             if log and (mi + 1) % max(1, models // 8) == 0:
                 log(f"pairs {k}/{n} ({time.perf_counter() - t0:.1f} s)")
     return X, T
+
+
+def _network_direction(ctx: api.Context, net: cnn.UNet, x) -> None:
+    """Set the context's search direction to the network's output for the
+    packed input x (the context's current accumulators and model)."""
+    torch = _torch()
+    d = ctx.dims
+    if "dir" not in _SCRATCH or _SCRATCH["dir"].numel() != d.nz * d.nx:
+        _SCRATCH["dir"] = torch.empty(d.nz * d.nx, dtype=torch.float32, device="cuda")
+    y = net.forward(x, 1, d.nx, d.nz)
+    cnn.direction(net, y, d.nz, d.nx, _SCRATCH["dir"])
+    torch.cuda.synchronize()
+    ctx.set_direction_dev(_SCRATCH["dir"].data_ptr())
 
 
 def train(net: cnn.UNet, X, T, setup: PairSetup = PairSetup(), epochs: int = 30, batch: int = 4, lr: float = 1e-3,
@@ -266,7 +290,8 @@ def time_to_error(log: FwiLog, target: float) -> float | None:
 def main(argv=None) -> int:
     """Train the preconditioner and compare CNN-preconditioned with plain FWI.
 
-    python -m fwi2d_b200.precond --models 128 --stages 4 --epochs 40 --iterations 10 --test small|aperture
+    python -m fwi2d_b200.precond --models 512 --stages 4 --epochs 60 --iterations 10 --test small|aperture
+        [--follow-stages 4 --follow-epochs 30]
     writes a JSON summary (--out) with the training history and both runs'
     misfit, model-error and wall-time trajectories."""
     import argparse
@@ -285,6 +310,10 @@ def main(argv=None) -> int:
     ap.add_argument("--target", type=float, default=0.03)
     ap.add_argument("--out", default=None)
     ap.add_argument("--weights", default=None, help="save / load the trained network here")
+    ap.add_argument("--follow-stages", type=int, default=0,
+                    help="after training, make this many more pairs per model along the network's own FWI "
+                         "trajectories and continue training on all pairs (0: off)")
+    ap.add_argument("--follow-epochs", type=int, default=30)
     a = ap.parse_args(argv)
     root = Path(tempfile.mkdtemp(prefix="fwi2d_precond_"))
     s = PairSetup()
@@ -300,6 +329,16 @@ def main(argv=None) -> int:
         hist = train(net, X, T, s, epochs=a.epochs, batch=4, lr=1e-3, val=8 * a.stages)
         t2 = time.perf_counter()
         res["training"] = {"pairs": int(X.shape[0]), "pair_seconds": t1 - t0, "train_seconds": t2 - t1, **hist}
+        if a.follow_stages > 0:
+            X2, T2 = make_pairs(root / "pairs_follow", a.models, a.follow_stages, setup=s, net=net)
+            X = torch.cat([X, X2])
+            T = torch.cat([T, T2])
+            del X2, T2
+            t3 = time.perf_counter()
+            hist2 = train(net, X, T, s, epochs=a.follow_epochs, batch=4, lr=5e-4, val=8 * a.stages, seed=1)
+            t4 = time.perf_counter()
+            res["training_follow"] = {"pairs": int(X.shape[0]), "pair_seconds": t3 - t2, "train_seconds": t4 - t3,
+                                      **hist2}
         del X, T
         if a.weights:
             net.save(a.weights)
