@@ -66,6 +66,17 @@ def test_cnn_direction_cuts_misfit_faster(trained):
     assert t_cnn < plain.seconds[-1], (t_cnn, plain.seconds)
 
 
+def test_pairs_along_the_network_trajectory(trained):
+    """make_pairs given a network steps each stage along the network's direction
+    (with the gradient fallback): finite inputs, targets normalised to max 1."""
+    root, net, _ = trained
+    X, T = precond.make_pairs(root / "follow", models=2, stages=2, setup=SETUP, log=None, net=net)
+    assert X.shape[0] == 4 and T.shape[0] == 4
+    assert bool(torch.isfinite(X.float()).all()) and bool(torch.isfinite(T).all())
+    for k in range(4):
+        assert abs(float(T[k].abs().max()) - 1.0) < 1e-6
+
+
 def test_training_models_are_held_out():
     """The pairs come from seeds TRAIN_SEED0 .. TRAIN_SEED0 + models - 1; the
     FWI test models (seeds 7 and 11 here, the 301 x 1701 model of seed 2 in
