@@ -212,6 +212,9 @@ def run_reference(args, rank, world):
             back = reference_backward(case, vp)
             if back:
                 line["backward_loops"] = back
+            fwi = reference_fwi_iteration()
+            if fwi:
+                line["fwi_iteration"] = fwi
     else:
         cb = cpu_baseline(case, vp)
         line.update(value=cb["value"], ms_per_step=None, cpu_baseline=dict(cb, kind="port"),
@@ -409,16 +412,12 @@ def fwi_surveys(iters_plain: int = 5, iters_batched: int = 1) -> dict:
     return out
 
 
-def reference_backward(case, vp, reps: int = 3) -> dict | None:
-    """The reference's own forward, migration and adjoint loops on the benchmark
-    geometry, run by oracle/_ref/ref_harness --time (built from the reference
-    sources; the boundary velocity is an input because the reference's
-    random-boundary kernels index out of bounds), CUDA events per loop."""
+def _harness_time(exe, case, vp, reps: int, seed: int = 1):
+    """Run oracle/_ref/ref_harness --time on `case` (boundary velocity: the
+    oracle's random boundary of the Gaussian-smoothed model, traces: seeded
+    noise) and return its per-repetition rows."""
     from fwi2d_b200 import synth
     from oracle import oracle as O
-    exe = ROOT / "oracle" / "_ref" / "ref_harness"
-    if not exe.exists():
-        return None
     nb = 100
     smooth = synth.smooth_model(vp, case.dh, 150.0)
     base = O.expand(smooth, nb)
@@ -426,7 +425,7 @@ def reference_backward(case, vp, reps: int = 3) -> dict | None:
     vel = O.rbc(base, nb, case.dh, 500.0, float(smooth.min()), float(smooth.max()), 0, 0, bt)
     vfile = case.root / "ref_vel.bin"
     np.ascontiguousarray(vel.T, dtype=np.float32).tofile(vfile)
-    rng = np.random.default_rng(1)
+    rng = np.random.default_rng(seed)
     for k in range(len(case.sx)):
         (rng.standard_normal(case.nt * len(case.rx)) * 1e-3).astype(np.float32).tofile(
             case.root / f"ref_data_{k + 1}.bin")
@@ -434,8 +433,48 @@ def reference_backward(case, vp, reps: int = 3) -> dict | None:
                        capture_output=True, text=True, cwd=str(case.root), timeout=900,
                        env=dict(os.environ, TERM=os.environ.get("TERM", "dumb")))
     if r.returncode != 0:
-        return {"error": f"ref_harness --time rc={r.returncode}: {r.stderr[-300:]}"}
-    rows = [dict(kv.split("=") for kv in ln.split()[1:]) for ln in r.stdout.splitlines() if ln.startswith("time ")]
+        raise RuntimeError(f"ref_harness --time rc={r.returncode}: {r.stderr[-300:]}")
+    return [dict(kv.split("=") for kv in ln.split()[1:]) for ln in r.stdout.splitlines() if ln.startswith("time ")]
+
+
+def reference_fwi_iteration() -> dict | None:
+    """The reference's FWI iteration on the 81-shot survey (301 x 1701 + 100-cell
+    boundaries, nt 4001), composed from its own loops timed once by
+    ref_harness: per shot the residual modeling and the two line-search
+    modelings (forward_solver, absorbing boundary on), the random-boundary
+    forward and the adjoint back-propagation (inversion.cu:111-166, 286-342).
+    Host work (file reads, the residual loop) is not included."""
+    from fwi2d_b200 import synth
+    exe = ROOT / "oracle" / "_ref" / "ref_harness"
+    if not exe.exists():
+        return None
+    d = Path(tempfile.mkdtemp(prefix="fwi2d_ref_fwi_"))
+    case, vp = synth.fwi_survey(d)
+    try:
+        row = _harness_time(exe, case, synth.gradient_model(vp, case.dh), reps=1)[0]
+    except (RuntimeError, subprocess.TimeoutExpired) as e:
+        return {"error": str(e)}
+    ms = 3 * float(row["fwd_abc_ms"]) + float(row["fwd_ms"]) + float(row["grad_bwd_ms"])
+    return {"workload": "the reference's loops on the 81-shot FWI survey: 501x1901 padded, nt 4001 + 237 levels",
+            "s_per_iteration": ms * 1e-3, "shots_per_s": len(case.sx) / (ms * 1e-3),
+            "composition": "3 x modeling forward (ABC) + random-boundary forward + adjoint back-propagation per "
+                           "shot, the reference's kernels only",
+            "modeling_forward_ms": float(row["fwd_abc_ms"]), "rbc_forward_ms": float(row["fwd_ms"]),
+            "adjoint_ms": float(row["grad_bwd_ms"]), "reference_build": "oracle/_ref/ref_harness"}
+
+
+def reference_backward(case, vp, reps: int = 3) -> dict | None:
+    """The reference's own forward, migration and adjoint loops on the benchmark
+    geometry, run by oracle/_ref/ref_harness --time (built from the reference
+    sources; the boundary velocity is an input because the reference's
+    random-boundary kernels index out of bounds), CUDA events per loop."""
+    exe = ROOT / "oracle" / "_ref" / "ref_harness"
+    if not exe.exists():
+        return None
+    try:
+        rows = _harness_time(exe, case, vp, reps)
+    except (RuntimeError, subprocess.TimeoutExpired) as e:
+        return {"error": str(e)}
     rows = rows[1:] if len(rows) > 1 else rows  # the first repetition warms up
     ups = float(rows[0]["updates"])
     mean = lambda k: float(np.mean([float(x[k]) for x in rows]))
@@ -444,6 +483,7 @@ def reference_backward(case, vp, reps: int = 3) -> dict | None:
             "forward_rbc": {"updates_per_s": ups / (mean("fwd_ms") * 1e-3), "ms": mean("fwd_ms")},
             "rtm_backward": {"updates_per_s": ups / (mean("rtm_bwd_ms") * 1e-3), "ms": mean("rtm_bwd_ms")},
             "gradient_backward": {"updates_per_s": ups / (mean("grad_bwd_ms") * 1e-3), "ms": mean("grad_bwd_ms")},
+            "modeling_forward": {"updates_per_s": ups / (mean("fwd_abc_ms") * 1e-3), "ms": mean("fwd_abc_ms")},
             "reference_build": "oracle/_ref/ref_harness", "repetitions_timed": len(rows)}
 
 

@@ -29,8 +29,10 @@
 //   (inject_seismogram + cross_correlation, migration.cu:61-81) and the
 //   adjoint back-propagation (inject_adjoint + build_gradient,
 //   inversion.cu:230-248); prints one line per repetition:
-//   "time fwd_ms=... rtm_bwd_ms=... grad_bwd_ms=... updates=..." where updates
-//   = shots x nxx x nzz x (nt + tlag) per propagation.
+//   "time fwd_ms=... rtm_bwd_ms=... grad_bwd_ms=... fwd_abc_ms=... updates=..."
+//   (fwd_abc: forward_solver with the absorbing boundary on, the modeling's
+//   propagation) where updates = shots x nxx x nzz x (nt + tlag) per
+//   propagation.
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -130,9 +132,12 @@ public:
             return (double)ms;
         };
         for (int r = 0; r < reps; ++r) {
-            double fwd = 0, rtm = 0, grad = 0;
+            double fwd = 0, rtm = 0, grad = 0, fwd_abc = 0;
             for (srcId = 0; srcId < geometry->nsrc; srcId++) {
                 initialization();
+                ABC = true;  // the modeling's propagation (absorbing boundary on)
+                fwd_abc += timed([&] { forward_solver(); });
+                ABC = false;
                 for (int mode = 0; mode < 2; ++mode) {
                     fwd += timed([&] { forward_solver(); });
                     cudaMemcpy(d_seismogram, data[srcId].data(), data[srcId].size() * sizeof(float),
@@ -146,8 +151,8 @@ public:
             }
             cudaError_t err = cudaDeviceSynchronize();
             if (err != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); std::exit(3); }
-            std::printf("time fwd_ms=%.4f rtm_bwd_ms=%.4f grad_bwd_ms=%.4f updates=%lld\n", fwd / 2, rtm, grad,
-                        (long long)geometry->nsrc * nxx * nzz * (nt + tlag));
+            std::printf("time fwd_ms=%.4f rtm_bwd_ms=%.4f grad_bwd_ms=%.4f fwd_abc_ms=%.4f updates=%lld\n", fwd / 2,
+                        rtm, grad, fwd_abc, (long long)geometry->nsrc * nxx * nzz * (nt + tlag));
             std::fflush(stdout);
         }
     }
