@@ -101,7 +101,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ in, int N, int H,
                                                                 int W, int Cin, const __nv_bfloat16* __restrict__ w,
                                                                 const float* __restrict__ bias, int Cout, int ncols,
-                                                                uint32_t stage_bytes, int nk, int relu,
+                                                                uint32_t stage_bytes, int relu,
                                                                 __nv_bfloat16* __restrict__ out,
                                                                 float* __restrict__ out32) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
     const int tid = threadIdx.x, warp = tid >> 5;
     const long long P = (long long)N * H * W;
     const long long p = (long long)blockIdx.x * kTcM + tid;  // this thread's pixel (A row, TMEM lane)
-    const uint32_t a_bytes = (uint32_t)kTcM * (Cin / nk) * 2;
+    const int kc = Cin / 8;
+    const uint32_t a_bytes = (uint32_t)kTcM * Cin * 2;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_slot)),
@@ -137,44 +138,39 @@ __global__ void __launch_bounds__(kTcThreads) conv3x3_tc_kernel(const __nv_bfloa
     }
     const uint32_t idesc = umma_idesc(kTcM, Cout);
     bool ok = true;
-    // steps: (tap, chunk of cc input channels); a small chunk keeps two
-    // stages small enough for several CTAs per SM
-    const int cc = Cin / nk, kcc = cc / 8, nsteps = 9 * nk;
-    for (int step = 0; step < nsteps; ++step) {
-        const int s = step & 1, tap = step / nk, h = step - tap * nk;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int s = tap & 1;
         unsigned char* A = smem + (size_t)s * stage_bytes;
         unsigned char* B = A + a_bytes;
-        // the stage's previous MMAs (step - 2) must be done before it is rewritten
-        if (step >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((step - 2) >> 1) & 1))) ok = false;
+        // the stage's previous MMAs (tap - 2) must be done before it is rewritten
+        if (tap >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((tap - 2) >> 1) & 1))) ok = false;
         const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
         const bool in_ok = valid && yy >= 0 && yy < H && xx >= 0 && xx < W;
         const uint4* src = reinterpret_cast<const uint4*>(in + (((long long)n * H + (in_ok ? yy : 0)) * W +
-                                                                (in_ok ? xx : 0)) * Cin) + h * kcc;
-        unsigned char* arow = A + (size_t)(tid >> 3) * kcc * 128 + (tid & 7) * 16;
+                                                                (in_ok ? xx : 0)) * Cin);
+        unsigned char* arow = A + (size_t)(tid >> 3) * kc * 128 + (tid & 7) * 16;
         const uint32_t a_src = in_ok ? 16u : 0u;
-        for (int j = 0; j < kcc; ++j) cp_async16(arow + (size_t)j * 128, src + j, a_src);
-        for (int e = tid; e < Cout * kcc; e += kTcThreads) {
-            const int co = e / kcc, j = e - co * kcc;
-            cp_async16(B + ((size_t)(co >> 3) * kcc + j) * 128 + (co & 7) * 16,
-                       reinterpret_cast<const uint4*>(w + ((long long)co * 9 + tap) * Cin) + h * kcc + j, 16u);
+        for (int j = 0; j < kc; ++j) cp_async16(arow + (size_t)j * 128, src + j, a_src);
+        for (int e = tid; e < Cout * kc; e += kTcThreads) {
+            const int co = e / kc, j = e - co * kc;
+            cp_async16(B + ((size_t)(co >> 3) * kc + j) * 128 + (co & 7) * 16,
+                       reinterpret_cast<const uint4*>(w + ((long long)co * 9 + tap) * Cin) + j, 16u);
         }
         cp_async_wait_all_async_proxy();  // the tensor cores read these copies through the async proxy
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
             const uint32_t sa = saddr(A), sb = saddr(B);
-            for (int k = 0; k < cc / 16; ++k)
-                umma_bf16(tmem, umma_desc(sa + 256u * k, 128u, (uint32_t)kcc * 128u),
-                          umma_desc(sb + 256u * k, 128u, (uint32_t)kcc * 128u), idesc, (step | k) != 0 ? 1u : 0u);
+            for (int k = 0; k < Cin / 16; ++k)
+                umma_bf16(tmem, umma_desc(sa + 256u * k, 128u, (uint32_t)kc * 128u),
+                          umma_desc(sb + 256u * k, 128u, (uint32_t)kc * 128u), idesc, (tap | k) != 0 ? 1u : 0u);
             umma_commit(&bar[s]);
         }
     }
-    // the last step commits after every earlier MMA; the last arrival on the
-    // other stage is collected too, so none lands after exit
-    for (int st = 0; st < 2 && st < nsteps; ++st) {
-        const int last = nsteps - 1 - ((nsteps - 1 - st) & 1);  // the last step on stage st
-        if (!tma::mbar_wait(&bar[st], (uint32_t)((last >> 1) & 1))) ok = false;
-    }
+    // tap 8 (stage 0, its 5th use) commits after every earlier MMA; the last
+    // arrival on stage 1 (tap 7) is collected too, so none lands after exit
+    if (!tma::mbar_wait(&bar[0], 0u)) ok = false;
+    if (!tma::mbar_wait(&bar[1], 1u)) ok = false;
     tc_fence_after();
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
     for (int c0 = 0; c0 < Cout; c0 += 8) {
@@ -357,12 +353,7 @@ int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, c
     if (Cin % 16 || Cin > 256 || Cout % 16 || Cout > 256 || N < 1 || H < 1 || W < 1) return -1;
     int ncols = 32;
     while (ncols < Cout) ncols *= 2;
-    // input channels per step: the fewest chunks (of a multiple of 16 channels)
-    // whose two stages fit in 100 KB, so that two or more CTAs share an SM
-    int nk = 1;
-    auto stage_of = [&](int k) { return ((uint32_t)(kTcM + Cout) * (uint32_t)(Cin / k) * 2u + 1023u) / 1024u * 1024u; };
-    while (2 * (size_t)stage_of(nk) > 100 * 1024 && Cin % (2 * nk) == 0 && (Cin / (2 * nk)) % 16 == 0) nk *= 2;
-    const uint32_t stage = stage_of(nk);
+    const uint32_t stage = ((uint32_t)(kTcM * Cin + Cout * Cin) * 2u + 1023u) / 1024u * 1024u;
     // at most 512 TMEM columns of resident CTAs per SM: ask for enough shared
     // memory that no more CTAs than that fit
     size_t smem = 2 * (size_t)stage;
@@ -384,7 +375,7 @@ int nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, c
     const unsigned grid = (unsigned)((P + kTcM - 1) / kTcM);
     conv3x3_tc_kernel<<<grid, kTcThreads, smem, st>>>(
         static_cast<const __nv_bfloat16*>(in), N, H, W, Cin, static_cast<const __nv_bfloat16*>(w), bias, Cout, ncols,
-        stage, nk, relu, static_cast<__nv_bfloat16*>(out), out32);
+        stage, relu, static_cast<__nv_bfloat16*>(out), out32);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
