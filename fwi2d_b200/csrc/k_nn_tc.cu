@@ -250,6 +250,13 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
     // M = 128, N = Cin, both operands MN-major (bits 15 and 16)
     const uint32_t idesc = umma_idesc(128, Cin) | (1u << 15) | (1u << 16);
     const int nstage = p_end > p_begin ? (int)((p_end - p_begin + kWgK - 1) / kWgK) : 0;
+    // the output-channel groups past Cout (M is padded to 128) hold zeros in
+    // both stages for the whole launch: cleared once here, never copied
+    const int mgroups = (Cout + 7) / 8;
+    for (int s = 0; s < 2; ++s) {
+        uint4* pad = reinterpret_cast<uint4*>(smem + (size_t)s * stage_bytes + (size_t)mgroups * 8 * 128);
+        for (int i = tid; i < (16 - mgroups) * 8 * 8; i += kTcThreads) pad[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     bool ok = true;
     for (int st = 0; st < nstage; ++st) {
         const int s = st & 1;
@@ -257,12 +264,12 @@ __global__ void __launch_bounds__(kTcThreads) wgrad_tc_kernel(const __nv_bfloat1
         unsigned char* B = A + a_bytes;
         if (st >= 2 && !tma::mbar_wait(&bar[s], (uint32_t)(((st - 2) >> 1) & 1))) ok = false;
         const long long q0 = p_begin + (long long)st * kWgK;
-        // A: dout rows (pixels) x co, 16 co groups x 64 pixels (zeros past the
-        // chunk and past Cout; the copy's source is then pixel p_begin, channel 0)
-        for (int e = tid; e < 16 * kWgK; e += kTcThreads) {
+        // A: dout rows (pixels) x co, the Cout / 8 real co groups x 64 pixels
+        // (zeros past the chunk; the copy's source is then pixel p_begin, channel 0)
+        for (int e = tid; e < mgroups * kWgK; e += kTcThreads) {
             const int mi = e / kWgK, r = e - mi * kWgK;  // co group, pixel in stage
             const long long q = q0 + r;
-            const bool ok_a = q < p_end && mi * 8 < Cout;
+            const bool ok_a = q < p_end;
             cp_async16(A + ((size_t)mi * 8 + (r >> 3)) * 128 + (r & 7) * 16,
                        reinterpret_cast<const uint4*>(dout + (ok_a ? q * Cout + mi * 8 : p_begin * Cout)),
                        ok_a ? 16u : 0u);
