@@ -38,7 +38,7 @@ extern "C" {
 #define FWI_ERR_IO       -2   /* file open / short read / write failure       */
 #define FWI_ERR_CUDA     -3   /* CUDA runtime error                           */
 #define FWI_ERR_CFL      -4   /* vmax*dt/dh above the 8th-order 2-D limit     */
-#define FWI_ERR_NAN      -5   /* non-finite wavefield or seismogram detected  */
+#define FWI_ERR_NAN      -5   /* non-finite wavefield, seismogram or misfit   */
 #define FWI_ERR_TIMEOUT  -6   /* a bounded device wait gave up                */
 #define FWI_ERR_STATE    -7   /* call out of order (e.g. gradient before data)*/
 #define FWI_ERR_ARG      -8   /* bad argument (NULL, shot out of range, size) */
@@ -131,7 +131,9 @@ int  fwi_set_observed(fwi_ctx* ctx, const float* obs_all);
 int  fwi_set_observed_dev(fwi_ctx* ctx, const float* d_obs_all);
 /* Inversion::compute_gradient (inversion.cu:111-166): ABC modeling, residual,
  * FP64 misfit, and - when with_gradient != 0 - RBC forward + adjoint back-
- * propagation + gradient post-processing.  *sum_res = sum of residual^2. */
+ * propagation + gradient post-processing.  *sum_res = sum of residual^2.
+ * A non-finite misfit (a model made unstable by an unbounded update) returns
+ * FWI_ERR_NAN where the reference would carry NaN on. */
 int  fwi_compute_gradient(fwi_ctx* ctx, int with_gradient, double* sum_res);
 /* ---- sharded inversion (shots split over processes / GPUs) ---------------
  * fwi_compute_gradient(ctx, 1, s) equals fwi_gradient_accumulate followed by
