@@ -238,6 +238,8 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
     up(&t->d_rec_col, rec_col, "receivers per column");
     t->h_src_colptr = std::move(src_colptr);
     t->h_rec_colptr = std::move(rec_colptr);
+    t->h_rec_ent_z = rec_z;
+    t->h_rec_ent_soff = rec_soff;
 }
 
 void Engine::free_tables(Tables* t) {
@@ -374,7 +376,8 @@ Engine::~Engine() {
                     d_batch_id_, d_batch_c0_, d_batch_w_, d_bump_ptr_, d_bumps_, fld_[0], fld_[1], fld_[2],
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
                     d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_, d_sync_,
-                    d_slabs_, d_xbuf_, d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_};
+                    d_slabs_, d_xbuf_, d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_,
+                    d_inj_ptr_, d_inj_pts_, d_inj_soff_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& r : timed_) {
@@ -1317,6 +1320,82 @@ Engine::BwdPlan Engine::bwd_plan(const Grid& g, const Tables& t, int ns, const f
     return best;
 }
 
+// Receiver points of the batch's shots per CTA of a multi-level backward
+// launch of `grid` CTAs over tx-column tiles: tiles are numbered as in
+// upload_tile_base (down the columns of a shot, shots in order) and CTA b owns
+// tiles b, b + grid, ...; entries at the same point stay together, in entry
+// order, so one thread adds them as the column-table walk did.
+void Engine::upload_injection_points(const Grid& g, const Tables& t, int ns, int tx, int grid) {
+    const int R = fwd_tma_rows();
+    const int ntz = (g.ldz + R - 1) / R;
+    const long long fs = g.fstride();
+    struct Rec {
+        int cta;
+        long long g;
+        int k;
+    };
+    std::vector<Rec> recs;
+    int tile0 = 0;
+    for (int s = 0; s < ns; ++s) {
+        const ShotDesc& sd = t.shots[batch_s0_ + s];
+        const int nxx = h_shot_nxx(g, s);
+        for (int j = 0; j < nxx; ++j) {
+            const int kb = t.h_rec_colptr[sd.col_off + j], ke = t.h_rec_colptr[sd.col_off + j + 1];
+            for (int k = kb; k < ke; ++k) {
+                const int z = t.h_rec_ent_z[k];
+                const int tile = tile0 + (j / tx) * ntz + z / R;
+                recs.push_back(Rec{tile % grid, (long long)s * fs + (long long)j * g.ldz + z, k});
+            }
+        }
+        tile0 += ntz * ((nxx + tx - 1) / tx);
+    }
+    std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
+        return a.cta != b.cta ? a.cta < b.cta : (a.g != b.g ? a.g < b.g : a.k < b.k);
+    });
+    h_inj_ptr_.assign((size_t)grid + 1, 0);
+    h_inj_pts_.clear();
+    h_inj_soff_.clear();
+    for (size_t i = 0; i < recs.size();) {
+        InjPoint pt;
+        pt.g = recs[i].g;
+        pt.e0 = (int)h_inj_soff_.size();
+        size_t e = i;
+        for (; e < recs.size() && recs[e].cta == recs[i].cta && recs[e].g == recs[i].g; ++e)
+            h_inj_soff_.push_back(t.h_rec_ent_soff[recs[e].k]);
+        pt.e1 = (int)h_inj_soff_.size();
+        h_inj_pts_.push_back(pt);
+        ++h_inj_ptr_[recs[i].cta + 1];
+        i = e;
+    }
+    for (int b = 0; b < grid; ++b) h_inj_ptr_[b + 1] += h_inj_ptr_[b];
+    auto grow = [&](auto** buf, size_t* cap, size_t need, const char* what) {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(*buf)>>;
+        need = std::max<size_t>(need, 1);
+        if (need > *cap) {
+            check(cudaStreamSynchronize(st_), "sync before injection-table realloc");
+            cudaFree(*buf);
+            *buf = nullptr;
+            *cap = 0;
+            *buf = dalloc<T>(need * 2, what);
+            *cap = need * 2;
+        }
+    };
+    grow(&d_inj_ptr_, &inj_ptr_cap_, h_inj_ptr_.size(), "injection CTA table");
+    grow(&d_inj_pts_, &inj_pts_cap_, h_inj_pts_.size(), "injection points");
+    grow(&d_inj_soff_, &inj_soff_cap_, h_inj_soff_.size(), "injection trace offsets");
+    check(cudaMemcpyAsync(d_inj_ptr_, h_inj_ptr_.data(), h_inj_ptr_.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          st_),
+          "upload injection CTA table");
+    if (!h_inj_pts_.empty()) {
+        check(cudaMemcpyAsync(d_inj_pts_, h_inj_pts_.data(), h_inj_pts_.size() * sizeof(InjPoint),
+                              cudaMemcpyHostToDevice, st_),
+              "upload injection points");
+        check(cudaMemcpyAsync(d_inj_soff_, h_inj_soff_.data(), h_inj_soff_.size() * sizeof(long long),
+                              cudaMemcpyHostToDevice, st_),
+              "upload injection trace offsets");
+    }
+}
+
 void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,
                                     long long vel_stride, bool gradient, const float* d_series, float* const ps[2],
                                     float* const pr[2], int b_begin, int b_end, long long timed_updates) {
@@ -1353,6 +1432,10 @@ void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Table
     a.pr[1] = pr[1];
     a.acc_a = acc_[0];
     a.acc_b = acc_[1];
+    upload_injection_points(g, t, ns, p.TX, p.grid);
+    a.inj_cta_ptr = d_inj_ptr_;
+    a.inj_pts = d_inj_pts_;
+    a.inj_soff = d_inj_soff_;
     a.err = d_err_;
     a.sync = d_sync_;
     a.spin = spin_limit_;

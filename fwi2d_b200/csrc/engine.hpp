@@ -120,6 +120,8 @@ private:
         long long* d_rec_soff = nullptr;
         RecCol* d_rec_col = nullptr;       // per shot column: receivers there (first one's row, trace)
         std::vector<int> h_src_colptr, h_rec_colptr;  // host copies of the column tables
+        std::vector<int> h_rec_ent_z;                  // host copies of the receiver entries' rows
+        std::vector<long long> h_rec_ent_soff;         // and trace offsets (indexed like d_rec_z)
     };
     enum Kind { kFwdRecord = 0, kFwdNoRecord = 1, kBwdImage = 2, kBwdGradient = 3 };
 
@@ -257,6 +259,15 @@ private:
     int* d_bump_ptr_ = nullptr;
     BumpDev* d_bumps_ = nullptr;
     size_t bumps_cap_ = 0;
+    // multi-level backward kernel: receiver points per CTA (built per launch)
+    int* d_inj_ptr_ = nullptr;
+    InjPoint* d_inj_pts_ = nullptr;
+    long long* d_inj_soff_ = nullptr;
+    size_t inj_ptr_cap_ = 0, inj_pts_cap_ = 0, inj_soff_cap_ = 0;
+    std::vector<int> h_inj_ptr_;
+    std::vector<InjPoint> h_inj_pts_;
+    std::vector<long long> h_inj_soff_;
+    void upload_injection_points(const Grid& g, const Tables& t, int ns, int tx, int grid);
     float* fld_[4] = {nullptr, nullptr, nullptr, nullptr};
     float* acc_[2] = {nullptr, nullptr};
     float* d_vel_batch_ = nullptr;   // per-shot RBC velocity

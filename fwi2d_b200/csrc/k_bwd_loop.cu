@@ -18,7 +18,13 @@
 //     source and receiver fields of the level before, both accumulators);
 //   * eight consumer warps compute from shared memory (thread = 4 rows of
 //     TX/8 columns, register-window Laplacians) and store the four outputs
-//     with coalesced float4 stores, then release the stage.
+//     with coalesced float4 stores, then release the stage;
+//   * the receivers' samples are injected after a CTA's tiles of the level
+//     are stored and before the grid barrier: the host lists, per CTA, the
+//     receiver points of its tiles (a CTA owns the same tiles at every
+//     level), and its threads add each point's samples with one
+//     read-modify-write, so no tile load or update waits on the receiver
+//     tables.
 //
 // Every wait is bounded (tma::kSpinLimit polls); a wait that gives up raises
 // *err and the kernel returns once its own copies in flight have landed.
@@ -58,7 +64,7 @@ struct BGeom {
 };
 
 struct BMeta {
-    int s, x0, z0, nxx, col_off, has_rec;
+    int s, x0, z0, nxx, col_off;
 };
 
 // Gives up after `limit` polls; the drill instantiation also gives up when
@@ -101,7 +107,7 @@ __device__ __forceinline__ ft::TileInfo decode_tile(const BwdLoopArgs& a, int ti
 
 // Consumer pass over one staged tile of level b.
 template <int TX, bool GRAD, bool EDGE>
-__device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stage, const BMeta& mt, int sample,
+__device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stage, const BMeta& mt,
                                          float* ps_out, float* pr_out) {
     using G = BGeom<TX>;
     constexpr int CPW = TX / 8;
@@ -136,8 +142,7 @@ __device__ __forceinline__ void bwd_tile(const BwdLoopArgs& a, const float* stag
         const bool colok = !EDGE || (gx >= 4 && gx < mt.nxx - 4);
         const st::Bwd4 r = st::bwd_update4<GRAD, EDGE>(ls[m], psold[m], lr[m], pr[m], ps, prold, vv, ga, gb,
                                                        a.dt2idh2, a.dt, a.idh2, rows, colok);
-        float4 rv = r.pr;
-        if (mt.has_rec) st::inject4(a.inj, sample, mt.col_off, gx, z, rv);
+        const float4 rv = r.pr;  // the receivers' samples are added at the end of the level
         const size_t g = so + (size_t)gx * a.ldz + z;
         *reinterpret_cast<float4*>(ps_out + g) = r.ps;
         *reinterpret_cast<float4*>(pr_out + g) = rv;
@@ -200,7 +205,6 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                     mt.z0 = z0;
                     mt.nxx = sd.nxx;
                     mt.col_off = sd.col_off;
-                    mt.has_rec = sample >= 0 && st::has_points(a.inj, sd.col_off, x0, min(x0 + TX, sd.nxx));
                     float* base = smem + stg * G::STAGE;
                     float* pts = base + 2 * G::ST;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
@@ -234,15 +238,31 @@ __global__ void __launch_bounds__(kNT, TX == 8 ? 2 : 1)
                 const BMeta mt = meta[stg];
                 const float* stage = smem + stg * G::STAGE;
                 if (st::tile_inner(mt.z0, kTZ, mt.x0, TX, a.nzz, mt.nxx))
-                    bwd_tile<TX, GRAD, false>(a, stage, mt, sample, ps_out, pr_out);
+                    bwd_tile<TX, GRAD, false>(a, stage, mt, ps_out, pr_out);
                 else
-                    bwd_tile<TX, GRAD, true>(a, stage, mt, sample, ps_out, pr_out);
+                    bwd_tile<TX, GRAD, true>(a, stage, mt, ps_out, pr_out);
                 __syncwarp();
                 if (lane == 0) tma::mbar_arrive(&empty[stg]);
             }
         }
-        // the CTA's tiles of level b are written: grid barrier
+        // the CTA's tiles of level b are written: the receiver points in them
+        // take this level's samples (one read-modify-write per point, its
+        // receivers in entry order), then the grid barrier
         __syncthreads();
+        if (sample >= 0) {
+            float* pr_out = a.pr[p ^ 1];
+            const int q1 = __ldg(a.inj_cta_ptr + blockIdx.x + 1);
+            for (int q = __ldg(a.inj_cta_ptr + blockIdx.x) + tid; q < q1; q += kNT) {
+                const InjPoint pt = a.inj_pts[q];
+                float v = pr_out[pt.g];
+                for (int e = pt.e0; e < pt.e1; ++e) {
+                    const float amp = a.inj.scale * __ldg(a.inj.series + __ldg(a.inj_soff + e) + sample);
+                    v += amp;
+                }
+                pr_out[pt.g] = v;
+            }
+            __syncthreads();
+        }
         if (tid == 0 && !abort_flag) {
             if (!grid_barrier<DRILL>(a.sync, (unsigned)(b - a.b_begin + 1) * gridDim.x, limit, a.err)) {
                 atomicExch(a.err, 1);

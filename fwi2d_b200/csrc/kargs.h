@@ -152,6 +152,14 @@ struct FwdTmaConfig {
 // field through the stencil from ps[(b+1)&1] and pointwise from ps[b&1] (and
 // overwrites it), the receiver field through the stencil from pr[b&1] and
 // pointwise from pr[(b+1)&1] (overwritten), as run_backward alternates them.
+// A grid point that receives injected samples in the multi-level backward
+// kernel: its offset in a batch field and its entries [e0, e1) of the
+// trace-offset list (several receivers can share a point).
+struct __align__(16) InjPoint {
+    long long g;
+    int e0, e1;
+};
+
 struct BwdLoopArgs {
     const ShotDesc* shots;
     const int* tile_base;     // prefix sums of tiles per shot (ns+1)
@@ -167,6 +175,12 @@ struct BwdLoopArgs {
     float* pr[2];
     float* acc_a;
     float* acc_b;
+    // receiver injection, per CTA: the points of the receivers in the CTA's
+    // tiles (inj_cta_ptr[b] .. inj_cta_ptr[b+1] of inj_pts) and the trace
+    // offsets of their entries; the series and scale are inj's
+    const int* inj_cta_ptr;
+    const InjPoint* inj_pts;
+    const long long* inj_soff;
     int* err;
     unsigned* sync;           // grid-barrier counter, zero at launch
     unsigned spin;            // polls of a bounded wait before it gives up
