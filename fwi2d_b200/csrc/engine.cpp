@@ -377,7 +377,7 @@ Engine::~Engine() {
                     fld_[3], acc_[0], acc_[1], d_vel_batch_, d_seis_, d_data_, d_res_, d_partial_, d_sum_,
                     d_flag_, d_gmax_, d_img_, d_illum_, d_grad_, d_tmp_, d_tile_base_, d_err_, d_sync_,
                     d_slabs_, d_xbuf_, d_full_win_, d_trace_keep_, d_geo_, d_shot_bits_, d_weights_,
-                    d_inj_ptr_, d_inj_pts_, d_inj_soff_};
+                    d_inj_ptr_, d_inj_pts_, d_inj_soff_, d_rec_ptr_, d_rec_pts_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& r : timed_) {
@@ -812,6 +812,9 @@ void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Table
     la.buf_free = 2;
     for (int i = 0; i < 4; ++i) la.bufs[i] = fld_[i];
     la.sync = d_sync_;
+    if (record) upload_record_points(g, t, ns, TX, p.grid);
+    la.rec_cta_ptr = d_rec_ptr_;
+    la.rec_pts = d_rec_pts_;
     check(cudaMemsetAsync(d_sync_, 0, sizeof(unsigned), st_), "memset grid barrier");
     TimedRegion r;
     if (timed_updates >= 0) timing_begin(&r);
@@ -1394,6 +1397,60 @@ void Engine::upload_injection_points(const Grid& g, const Tables& t, int ns, int
                               cudaMemcpyHostToDevice, st_),
               "upload injection trace offsets");
     }
+}
+
+// Receiver entries of the batch's shots per CTA of a multi-level forward
+// launch (tiles numbered as in upload_tile_base, CTA b owns tiles b, b + grid,
+// ...), in entry order within a CTA.
+void Engine::upload_record_points(const Grid& g, const Tables& t, int ns, int tx, int grid) {
+    const int R = fwd_tma_rows();
+    const int ntz = (g.ldz + R - 1) / R;
+    const long long fs = g.fstride();
+    std::vector<std::pair<int, RecPoint>> recs;
+    int tile0 = 0;
+    for (int s = 0; s < ns; ++s) {
+        const ShotDesc& sd = t.shots[batch_s0_ + s];
+        const int nxx = h_shot_nxx(g, s);
+        for (int j = 0; j < nxx; ++j) {
+            const int kb = t.h_rec_colptr[sd.col_off + j], ke = t.h_rec_colptr[sd.col_off + j + 1];
+            for (int k = kb; k < ke; ++k) {
+                const int z = t.h_rec_ent_z[k];
+                const int tile = tile0 + (j / tx) * ntz + z / R;
+                recs.emplace_back(tile % grid,
+                                  RecPoint{(long long)s * fs + (long long)j * g.ldz + z, t.h_rec_ent_soff[k], z, j, nxx, 0});
+            }
+        }
+        tile0 += ntz * ((nxx + tx - 1) / tx);
+    }
+    std::stable_sort(recs.begin(), recs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    h_rec_ptr_.assign((size_t)grid + 1, 0);
+    h_rec_pts_.clear();
+    for (const auto& r : recs) {
+        ++h_rec_ptr_[r.first + 1];
+        h_rec_pts_.push_back(r.second);
+    }
+    for (int b = 0; b < grid; ++b) h_rec_ptr_[b + 1] += h_rec_ptr_[b];
+    auto grow = [&](auto** buf, size_t* cap, size_t need, const char* what) {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(*buf)>>;
+        need = std::max<size_t>(need, 1);
+        if (need > *cap) {
+            check(cudaStreamSynchronize(st_), "sync before record-table realloc");
+            cudaFree(*buf);
+            *buf = nullptr;
+            *cap = 0;
+            *buf = dalloc<T>(need * 2, what);
+            *cap = need * 2;
+        }
+    };
+    grow(&d_rec_ptr_, &rec_ptr_cap_, h_rec_ptr_.size(), "record CTA table");
+    grow(&d_rec_pts_, &rec_pts_cap_, h_rec_pts_.size(), "record points");
+    check(cudaMemcpyAsync(d_rec_ptr_, h_rec_ptr_.data(), h_rec_ptr_.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          st_),
+          "upload record CTA table");
+    if (!h_rec_pts_.empty())
+        check(cudaMemcpyAsync(d_rec_pts_, h_rec_pts_.data(), h_rec_pts_.size() * sizeof(RecPoint),
+                              cudaMemcpyHostToDevice, st_),
+              "upload record points");
 }
 
 void Engine::launch_bwd_loop_levels(const BwdPlan& p, const Grid& g, const Tables& t, int ns, const float* vel,

@@ -268,6 +268,13 @@ private:
     std::vector<InjPoint> h_inj_pts_;
     std::vector<long long> h_inj_soff_;
     void upload_injection_points(const Grid& g, const Tables& t, int ns, int tx, int grid);
+    // multi-level forward kernel: receiver entries per CTA (built per launch)
+    int* d_rec_ptr_ = nullptr;
+    RecPoint* d_rec_pts_ = nullptr;
+    size_t rec_ptr_cap_ = 0, rec_pts_cap_ = 0;
+    std::vector<int> h_rec_ptr_;
+    std::vector<RecPoint> h_rec_pts_;
+    void upload_record_points(const Grid& g, const Tables& t, int ns, int tx, int grid);
     float* fld_[4] = {nullptr, nullptr, nullptr, nullptr};
     float* acc_[2] = {nullptr, nullptr};
     float* d_vel_batch_ = nullptr;   // per-shot RBC velocity

@@ -113,13 +113,7 @@ __global__ void __launch_bounds__(kNT, MINB)
                     mt.col_off = sd.col_off;
                     mt.has_src = a.sample1 >= 0 &&
                                  st::has_points(a.inj, sd.col_off, ti.x0, min(ti.x0 + TX, sd.nxx));
-                    // receivers whose rows lie in the tile (surface receivers: the top tile of a strip)
-                    if (a.rec_sample0 >= 0 && a.seis && ti.z0 <= sd.rec_zmax && ti.z0 + kTZ > sd.rec_zmin) {
-                        mt.rec_kb = __ldg(a.rec.colptr + sd.col_off + ti.x0);
-                        mt.rec_ke = __ldg(a.rec.colptr + sd.col_off + min(ti.x0 + TX, sd.nxx));
-                    } else {
-                        mt.rec_kb = mt.rec_ke = 0;
-                    }
+                    mt.rec_kb = mt.rec_ke = 0;  // receivers are recorded at the end of the level
                     float* base = smem + stg * G::STAGE;
                     tma::mbar_arrive_expect_tx(&full[stg], G::BYTES);
                     tma::load_3d(base, &maps.cur[c], ti.z0 - 4, ti.x0 - 4, ti.s, &full[stg]);
@@ -157,26 +151,6 @@ __global__ void __launch_bounds__(kNT, MINB)
                 tl.mid = nullptr;
                 tl.has_src = mt.has_src != 0;
                 const float* b1d = ABC ? a.b1d : nullptr;
-                if (mt.rec_kb < mt.rec_ke) {
-                    // one thread per column of the tile: the column's receivers
-                    // from the per-column table (one load), more than one
-                    // receiver in a column from the column table
-                    const int xe = min(tl.ti.x0 + TX, tl.nxx);
-                    for (int x = tl.ti.x0 + tid; x < xe; x += kNC) {
-                        const int4 rc = __ldg(reinterpret_cast<const int4*>(a.rec_col + tl.col_off + x));
-                        const int kb = rc.y > 1 ? __ldg(a.rec.colptr + tl.col_off + x) : 0;
-                        for (int q = 0; q < rc.y; ++q) {
-                            const int z = q == 0 ? rc.x : __ldg(a.rec.z + kb + q);
-                            if (z < tl.ti.z0 || z >= tl.ti.z0 + kTZ) continue;
-                            const long long soff = q == 0 ? (((long long)(unsigned)rc.w << 32) | (unsigned)rc.z)
-                                                          : __ldg(a.rec.soff + kb + q);
-                            const float d = ABC ? st::damp(st::rows_info(a.b1d, a.nb, z, a.nzz),
-                                                           st::col_info(a.b1d, a.nb, x, tl.nxx), 0)
-                                                : 1.0f;
-                            a.seis[soff + a.rec_sample0] = d * tl.cur[(x - tl.ti.x0 + 4) * G::CZ + (z - tl.ti.z0 + 4)];
-                        }
-                    }
-                }
                 const bool inner = st::tile_inner(tl.ti.z0, kTZ, tl.ti.x0, TX, a.nzz, tl.nxx);
                 const bool undamped = st::tile_undamped(b1d, a.nb, tl.ti.z0, kTZ, tl.ti.x0, TX, a.nzz, tl.nxx);
                 if (inner && undamped) final_pass<1, TX, false, false>(a, tl);
@@ -186,7 +160,21 @@ __global__ void __launch_bounds__(kNT, MINB)
                 if (lane == 0) tma::mbar_arrive(&empty[stg]);
             }
         }
-        // the CTA's tiles of level t are written: grid barrier
+        // the CTA's tiles of level t are written; its receivers record Q^t,
+        // which stays in buffer c until level t + 2 writes there (the damper
+        // of the absorbing boundary as in compute_seismogram's ABC run);
+        // then the grid barrier
+        if (la.record && t > la.tlag && b.seis) {
+            const float* qt = la.bufs[c];
+            const int r1 = __ldg(la.rec_cta_ptr + blockIdx.x + 1);
+            for (int r = __ldg(la.rec_cta_ptr + blockIdx.x) + tid; r < r1; r += kNT) {
+                const RecPoint rp = la.rec_pts[r];
+                const float d = ABC ? st::damp(st::rows_info(b.b1d, b.nb, rp.z, b.nzz),
+                                               st::col_info(b.b1d, b.nb, rp.x, rp.nxx), 0)
+                                    : 1.0f;
+                b.seis[rp.soff + (t - la.tlag)] = d * __ldcg(qt + rp.g);
+            }
+        }
         __syncthreads();
         if (tid == 0 && !abort_flag) {
             if (!grid_barrier(la.sync, (unsigned)(t - la.t_begin + 1) * gridDim.x, b.spin, b.err)) {

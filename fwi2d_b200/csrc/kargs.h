@@ -97,6 +97,15 @@ struct FwdTmaArgs {
                               // tile and its grid-barrier arrival (-1: none)
 };
 
+// A receiver entry recorded by the multi-level forward kernel: its point's
+// offset in a batch field, its trace offset, its row and column in its shot's
+// grid and that grid's width (for the damper of the absorbing boundary).
+struct __align__(16) RecPoint {
+    long long g;
+    long long soff;
+    int z, x, nxx, pad;
+};
+
 // Cooperative multi-level forward kernel (k_fwd_loop.cu): levels
 // t_begin..t_end-1 in one launch, buffers rotating cur -> old, free -> cur.
 struct FwdLoopArgs {
@@ -106,6 +115,10 @@ struct FwdLoopArgs {
     int buf_cur, buf_old, buf_free;  // indices into bufs at t_begin
     float* bufs[4];
     unsigned* sync;           // grid-barrier counter, zero at launch
+    // receivers, per CTA: the entries in the CTA's tiles (rec_cta_ptr[b] ..
+    // rec_cta_ptr[b+1] of rec_pts), recorded at the end of each level
+    const int* rec_cta_ptr;
+    const RecPoint* rec_pts;
 };
 
 // Shared-memory-resident forward kernel (k_fwd_res.cu): CTA b owns slab b,
