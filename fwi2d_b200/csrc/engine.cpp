@@ -174,7 +174,6 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
     t->shots.resize(nsrc_);
     std::vector<int> rec_pt, rec_colptr, rec_z, src_colptr, src_z(nsrc_);
     std::vector<long long> rec_soff, src_soff(nsrc_, 0);
-    std::vector<RecCol> rec_col;
     for (int s = 0; s < nsrc_; ++s) {
         const int nxx = t->nxx[s], c0 = win_[s].c0;
         ShotDesc& d = t->shots[s];
@@ -183,8 +182,6 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
         d.col_off = (int)src_colptr.size();
         d.seis_off = (long long)s * nrec_ * nt_;
         d.vel_col = 0;
-        d.rec_zmin = INT32_MAX;
-        d.rec_zmax = INT32_MIN;
         // source: one entry per shot, in the shot's own column table
         src_z[s] = t->src_z[s];
         const int sx = t->src_x[s] - c0;
@@ -207,19 +204,6 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
             rec_z.push_back(t->rec_z[r]);
             rec_pt.push_back(t->rec_z[r] + (t->rec_x[r] - c0) * g->ldz);
             rec_soff.push_back(d.seis_off + (long long)r * nt_);
-            d.rec_zmin = std::min(d.rec_zmin, t->rec_z[r]);
-            d.rec_zmax = std::max(d.rec_zmax, t->rec_z[r]);
-        }
-        // per column: the number of receivers and the first one's row and trace
-        for (int j = 0; j <= nxx; ++j) {
-            const int kb = rec_colptr[d.col_off + j];
-            const int ke = j < nxx ? rec_colptr[d.col_off + j + 1] : kb;
-            RecCol rc{0, ke - kb, 0};
-            if (ke > kb) {
-                rc.z = rec_z[kb];
-                rc.soff = rec_soff[kb];
-            }
-            rec_col.push_back(rc);
         }
     }
     auto up = [&](auto** dst, const auto& v, const char* what) {
@@ -235,7 +219,6 @@ void Engine::setup_grid(Grid* g, Tables* t, int nb) {
     up(&t->d_rec_colptr, rec_colptr, "receiver columns");
     up(&t->d_rec_z, rec_z, "receiver rows");
     up(&t->d_rec_soff, rec_soff, "receiver offsets");
-    up(&t->d_rec_col, rec_col, "receivers per column");
     t->h_src_colptr = std::move(src_colptr);
     t->h_rec_colptr = std::move(rec_colptr);
     t->h_rec_ent_z = rec_z;
@@ -250,7 +233,6 @@ void Engine::free_tables(Tables* t) {
     cudaFree(t->d_rec_colptr);
     cudaFree(t->d_rec_z);
     cudaFree(t->d_rec_soff);
-    cudaFree(t->d_rec_col);
 }
 
 void Engine::alloc_buffers() {
@@ -686,7 +668,6 @@ void Engine::launch_fwd_tma_step(const FwdPlan& p, bool two, const Grid& g, cons
     a.sample1 = (tt + 1 < nt_) ? tt + 1 : -1;
     a.sample2 = (two && tt + 2 < nt_) ? tt + 2 : -1;
     a.rec = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, nullptr, -1, 0.0f};
-    a.rec_col = t.d_rec_col;
     a.seis = record ? d_seis : nullptr;
     a.rec_sample0 = (record && tt > tlag_) ? tt - tlag_ : -1;
     a.rec_sample1 = (record && two && tt + 1 > tlag_) ? tt + 1 - tlag_ : -1;
@@ -795,7 +776,6 @@ void Engine::launch_fwd_loop_levels(const FwdPlan& p, const Grid& g, const Table
     a.inj = InjTable{t.d_src_colptr, t.d_src_z, t.d_src_soff, d_wavelet_, -1, idh2_};
     a.sample1 = a.sample2 = -1;
     a.rec = InjTable{t.d_rec_colptr, t.d_rec_z, t.d_rec_soff, nullptr, -1, 0.0f};
-    a.rec_col = t.d_rec_col;
     a.seis = record ? d_seis : nullptr;
     a.rec_sample0 = a.rec_sample1 = -1;
     a.out1 = a.out2 = nullptr;

@@ -118,7 +118,6 @@ private:
         int* d_rec_colptr = nullptr;       // nsrc*(nxx+1)
         int* d_rec_z = nullptr;            // nsrc*nrec, sorted by column
         long long* d_rec_soff = nullptr;
-        RecCol* d_rec_col = nullptr;       // per shot column: receivers there (first one's row, trace)
         std::vector<int> h_src_colptr, h_rec_colptr;  // host copies of the column tables
         std::vector<int> h_rec_ent_z;                  // host copies of the receiver entries' rows
         std::vector<long long> h_rec_ent_soff;         // and trace offsets (indexed like d_rec_z)

@@ -28,17 +28,6 @@ struct ShotDesc {
     long long seis_off;  // float offset of the shot's nt x nrec trace-major block
     int vel_col;         // column of the velocity array that is column 0 of the
                          // shot's grid (aperture window over a shared velocity)
-    int rec_zmin, rec_zmax;  // rows of the shot's receivers (zmin > zmax: none)
-};
-
-// Receivers of one grid column of a shot (entry col_off + x, as the receiver
-// column table): how many, and the row and trace offset of the first.  The
-// multi-level forward kernel records from it instead of walking the column
-// table.
-struct __align__(16) RecCol {
-    int z;
-    int n;
-    long long soff;
 };
 
 // Point injections into the field written by a step (the source of a forward
@@ -86,7 +75,6 @@ struct FwdTmaArgs {
     InjTable inj;             // source table; sample1 / sample2 below
     int sample1, sample2;     // wavelet samples added to Q^{t+1}, Q^{t+2}; -1 none
     InjTable rec;             // receiver table (colptr, z, soff) of the batch
-    const RecCol* rec_col;    // per-column receivers (indexed like rec.colptr)
     float* seis;              // trace-major seismograms, NULL when not recording
     int rec_sample0, rec_sample1;  // samples recorded from Q^t and Q^{t+1}; -1 none
     float* out1;              // Q^{t+1}
