@@ -39,7 +39,7 @@ CU_SOURCES = {
     "k_bwd_loop.cu": [],
     "k_prep.cu": ["-fmad=false"],
     "k_nn.cu": [],
-    "k_nn_tc.cu": [],
+    "k_nn_tma.cu": [],
     "k_util.cu": [],
     "k_rbc.cu": ["-fmad=false"],
     "k_noalloc.cu": [],

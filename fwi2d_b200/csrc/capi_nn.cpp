@@ -16,7 +16,7 @@ extern "C" {
 int fwi_nn_conv3x3(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
                    int relu, void* out_bf16, float* out_f32, void* stream) {
     if (!in || !w || (!out_bf16 && !out_f32) || !dims_ok(N, H, W)) return FWI_ERR_ARG;
-    const int rc = fwi::nn_conv3x3_tc(in, N, H, W, Cin, w, bias, Cout, relu, out_bf16, out_f32, S(stream));
+    const int rc = fwi::nn_conv3x3_tma(in, N, H, W, Cin, w, bias, Cout, relu, out_bf16, out_f32, S(stream));
     if (rc == -1) return FWI_ERR_ARG;
     if (rc != 0) return FWI_ERR_CUDA;
     return status();
@@ -32,13 +32,17 @@ int fwi_nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void*
 
 int fwi_nn_check(void) {
     if (cudaDeviceSynchronize() != cudaSuccess) return FWI_ERR_CUDA;
-    const int e = fwi::nn_tc_error(true);
+    const int e = fwi::nn_tma_error(true);
     if (e < 0) return FWI_ERR_CUDA;
     return e ? FWI_ERR_TIMEOUT : FWI_OK;
 }
 
 size_t fwi_nn_wgrad_partial_floats(int N, int H, int W, int Cin, int Cout) {
-    return (size_t)fwi::nn_wgrad_chunks((long long)N * H * W) * (size_t)Cout * 9 * Cin;
+    // the larger of the mma.sync path's [chunk][co][tap][ci] and the tcgen05
+    // path's, which adds the [chunk][co] bias partials
+    const size_t mma = (size_t)fwi::nn_wgrad_chunks((long long)N * H * W) * (size_t)Cout * 9 * Cin;
+    const size_t tc = fwi::nn_wgrad_tma_partial_floats(N, H, W, Cin, Cout);
+    return mma > tc ? mma : tc;
 }
 
 int fwi_nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,

@@ -453,21 +453,28 @@ int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int 
     const int chunk = (int)(((P + chunks - 1) / chunks + 15) / 16 * 16);
     const auto* i16 = static_cast<const __nv_bfloat16*>(in);
     const auto* d16 = static_cast<const __nv_bfloat16*>(dout);
-    // the tcgen05 kernel takes up to 128 output channels; wider layers, and
-    // callers asking for the mma.sync path, use the warp-level kernel
-    const int tc = (tensor_memory && Cout <= 128) ? nn_wgrad_tc(in, dout, N, H, W, Cin, Cout, chunks, chunk, partial, st)
-                                                  : -1;
-    if (tc == -2) return -2;
-    if (tc != 0) {
-        if (Cin % 32 == 0) {
-            dim3 grid(chunks, 9, (Cout / 16) * (Cin / 32));
-            wgrad_kernel<4><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
-        } else {
-            dim3 grid(chunks, 9, (Cout / 16) * (Cin / 16));
-            wgrad_kernel<2><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+    const size_t nw = (size_t)Cout * 9 * Cin;
+    // the tcgen05 kernel takes up to 128 output channels and sums the bias
+    // gradient too; wider layers, and callers asking for the mma.sync path,
+    // use the warp-level kernel
+    if (tensor_memory && Cout <= 128) {
+        const int tc_chunks = nn_wgrad_tma(in, dout, N, H, W, Cin, Cout, partial, db != nullptr, st);
+        if (tc_chunks == -2) return -2;
+        if (tc_chunks > 0) {
+            wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, tc_chunks, nw, dw);
+            if (db)
+                wgrad_reduce_kernel<<<grid_n((size_t)Cout), 256, 0, st>>>(partial + (size_t)tc_chunks * nw, tc_chunks,
+                                                                          (size_t)Cout, db);
+            return 0;
         }
     }
-    const size_t nw = (size_t)Cout * 9 * Cin;
+    if (Cin % 32 == 0) {
+        dim3 grid(chunks, 9, (Cout / 16) * (Cin / 32));
+        wgrad_kernel<4><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+    } else {
+        dim3 grid(chunks, 9, (Cout / 16) * (Cin / 16));
+        wgrad_kernel<2><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
+    }
     wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, chunks, nw, dw);
     if (db) {
         if (256 % Cout == 0) {  // the chunk partials are consumed: reuse the scratch

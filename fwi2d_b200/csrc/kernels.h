@@ -134,11 +134,17 @@ void launch_smooth_slowness(const float* vp, int nz, int nx, const double* weigh
                             float* tmp, float* out, cudaStream_t st);
 
 // ---- k_nn.cu (CNN preconditioner; bf16 buffers passed as void*) ----------------
-// tcgen05 / TMEM implicit GEMM (k_nn_tc.cu): Cin, Cout multiples of 16, <= 256
-int  nn_conv3x3_tc(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
-                   void* out, float* out32, cudaStream_t st);
-// 1 when a bounded wait of the tcgen05 convolution gave up since the last reset
-int  nn_tc_error(bool reset);
+// TMA-fed, warp-specialised tcgen05 kernels (k_nn_tma.cu): the convolution
+// (Cin, Cout multiples of 16, <= 256) and the weight-gradient chunk partials
+// (Cout <= 128; returns the number of chunks, -1 for unsupported sizes);
+// partial holds [chunk][co][tap][ci] then, when bias, [chunk][co];
+// nn_tma_error: 1 when a bounded wait of either kernel gave up since the last reset
+int  nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
+                    int relu, void* out, float* out32, cudaStream_t st);
+size_t nn_wgrad_tma_partial_floats(int N, int H, int W, int Cin, int Cout);
+int  nn_wgrad_tma(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial, bool bias,
+                  cudaStream_t st);
+int  nn_tma_error(bool reset);
 // mma.sync m16n8k16 implicit GEMM (k_nn.cu)
 int  nn_conv3x3_mma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout,
                     int relu, void* out, float* out32, cudaStream_t st);
@@ -146,8 +152,6 @@ int  nn_wgrad_chunks(long long P);
 // tensor_memory: chunk partials on the tcgen05 kernel (Cout <= 128), else mma.sync
 int  nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
                       float* dw, float* db, cudaStream_t st, bool tensor_memory = true);
-int  nn_wgrad_tc(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, int chunks, int chunk,
-                 float* partial, cudaStream_t st);
 void nn_weight_prep(const float* w, int Cout, int Cin, void* wb, void* wt, cudaStream_t st);
 void nn_pool_fwd(const void* in, int N, int H, int W, int C, void* out, cudaStream_t st);
 void nn_pool_bwd(const float* dout, int N, int H, int W, int C, float* din, int accumulate, cudaStream_t st);

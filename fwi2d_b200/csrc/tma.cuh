@@ -76,5 +76,16 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* m, int c0,
         : "memory");
 }
 
+// 4-D tiled load of box (c0, c1, c2, c3); c0 is the contiguous coordinate and
+// must start on a 16-byte boundary.
+__device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* m, int c0, int c1, int c2, int c3,
+                                        uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+        : "memory");
+}
+
 }  // namespace tma
 }  // namespace fwi

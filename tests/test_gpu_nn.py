@@ -300,9 +300,13 @@ def test_tcgen05_and_mma_sync_weight_gradients_agree(N, H, W, Cin, Cout):
         res.append((dw, db))
     assert L.fwi_nn_check() == 0
     assert rel(res[0][0], res[1][0]) < 1e-5
-    assert torch.equal(res[0][1], res[1][1])
+    # the tcgen05 path sums the bias gradient on the tensor cores (an MMA
+    # against a block of ones), the mma.sync path per pixel chunk: same sums,
+    # another order
+    assert rel(res[0][1], res[1][1]) < 1e-6
     # and both against torch
     xr = nhwc_to_nchw(x.float().cpu(), N, H, W, Cin)
     dyr = nhwc_to_nchw(dy.float().cpu(), N, H, W, Cout)
     ref = torch.nn.grad.conv2d_weight(xr, (Cout, Cin, 3, 3), dyr, padding=1)
     assert rel(w_to_torch(res[0][0].cpu(), Cout, Cin), ref) < 1e-5
+    assert rel(res[0][1].cpu(), dyr.double().sum(dim=(0, 2, 3))) < 1e-6
