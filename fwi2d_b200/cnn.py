@@ -8,10 +8,10 @@ output replaces that direction (fwi_set_direction_dev) before the same
 the iteration falls back to the plain gradient.
 
 Every operation of the network runs in the project's own kernels
-(include/fwi2d_nn.h: 3x3 convolutions on the tcgen05 tensor cores with the
-FP32 accumulator in tensor memory, weight gradients on mma.sync, pooling,
-upsampling + skip concatenation, ReLU gradient, MSE, Adam); torch only
-allocates device memory.
+(include/fwi2d_nn.h: 3x3 convolutions and their weight and bias gradients on
+the tcgen05 tensor cores, operands loaded by TMA, FP32 accumulators in tensor
+memory; pooling, upsampling + skip concatenation, ReLU gradient, MSE, Adam);
+torch only allocates device memory.
 
 Architecture (channels c = 16, 32, 64, 128; every conv 3x3, ReLU but the last):
   enc1 3->16->16 | pool | enc2 16->32->32 | pool | enc3 32->64->64 | pool |

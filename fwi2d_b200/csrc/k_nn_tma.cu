@@ -1,32 +1,34 @@
 // k_nn_tma.cu — the U-Net's 3x3 convolutions and weight gradients on the
-// 5th-generation tensor cores, operands brought in by TMA, warp-specialised.
+// 5th-generation tensor cores, operands brought in by TMA, warp-specialised:
+// warp 0 (one lane) issues the TMA loads into a ring of mbarrier stages,
+// warp 1 (one lane) the `tcgen05.mma.kind::f16` (BF16 x BF16 -> FP32 in
+// tensor memory) and the commits, warps 2-5 read the accumulators back with
+// `tcgen05.ld.32x32b` (each its 32-lane quarter).  CTAs are persistent, one
+// per SM.  Every fixed cost here is per instruction of one thread (about
+// 60 ns a TMA load, 30 ns an MMA on this part), so the kernels are shaped to
+// issue few, wide operations per pixel.
 //
-// Convolution (forward and data gradient), implicit GEMM
-//   D[p, co] = sum_{tap, ci} in[p shifted by the tap, ci] w[co, tap, ci]:
-//   * an M tile is a bw x bh box of 128 pixels of one image (bw * bh = 128,
-//     chosen per layer to waste the fewest padded pixels); N = Cout <= 256;
-//     K runs over 9 taps x Cin in channel blocks of cb = 64, 32 or 16
-//     (128-, 64- or 32-byte rows, the matching TMA / UMMA swizzle);
-//   * warp 0 (one lane) issues, per (tap, channel block), one 4-D TMA load of
-//     the shifted pixel box (zero fill outside the image gives the padding)
-//     and one 3-D load of the tap's weights into a ring of stages;
-//   * warp 1 (one lane) issues the cb / 16 `tcgen05.mma.kind::f16` of each
-//     stage into one of two TMEM accumulators (M = 128 lanes x Cout columns)
-//     and commits the stage back to the producer; after a tile's last stage it
-//     commits the accumulator to the epilogue;
-//   * warps 2-5 read their 32 TMEM lanes each (`tcgen05.ld.32x32b`), add the
-//     bias, apply the ReLU and store NHWC rows, while the MMAs of the next tile
-//     run into the other accumulator.
-//   CTAs are persistent (one per SM, tiles round-robin).
+// Convolution D[p, co] = sum_{tap, ci} in[p + tap, ci] w[co, tap, ci], two kernels:
+//   * conv3x3_halo_kernel (the weights fit in shared memory next to the
+//     ring): a tile is 8 x 16 pixels; its input plus a one-pixel border is
+//     loaded once, one box per 8-channel plane, in the no-swizzle canonical
+//     layout, and the nine taps read it through shifted descriptors; the
+//     weights stay resident for the CTA's life;
+//   * conv3x3_tma_kernel (large weights): a tile is a bw x bh box of 128
+//     pixels; per (tap, channel block of 64 / 32 / 16) one swizzled 4-D box of
+//     the shifted pixels (zero fill gives the padding) and one of the weights.
+//   Both keep two TMEM accumulators (M = 128 lanes x Cout columns) so the
+//   epilogue of a tile (bias, ReLU, NHWC store) overlaps the next tile's MMAs.
 //
 // Weight gradient dW[co, tap, ci] = sum_p dout[p, co] in[p + tap, ci]:
-//   M = co (128 TMEM lanes; rows past Cout are ignored), N = ci, K = pixels in
-//   64-pixel boxes.  CTA (chunk, tap group) streams the boxes of its pixel
-//   chunk: per stage one dout box (MN-major A) and one shifted input box per
-//   tap of its group (MN-major B); every tap of the group accumulates in its
-//   own TMEM columns, and the bias gradient rides along as one more MMA against
-//   a block of ones.  The partials [chunk][co][tap][ci] and [chunk][co] are
-//   summed over chunks in a fixed order afterwards (deterministic).
+//   M = co (128 TMEM lanes; rows past Cout are ignored), K = pixels in boxes of
+//   128.  CTA (chunk, tap group) streams the boxes of its pixel chunk: per
+//   stage one output-gradient box (MN-major A) and one shifted input box per
+//   tap of its group (MN-major B).  The taps' input boxes sit back to back, so
+//   up to 256 / Cin taps form one MMA (N = taps x Cin) whose accumulator
+//   columns come out in [tap][ci] order; the bias gradient rides along as one
+//   more MMA against a block of ones.  The partials [chunk][co][tap][ci] and
+//   [chunk][co] are summed over chunks in a fixed order afterwards.
 //
 // Every wait is bounded (tma::kSpinLimit polls); a wait that gives up raises
 // g_nn_tma_err (fwi_nn_check), the roles stop issuing, the producer collects
@@ -48,7 +50,7 @@ namespace {
 constexpr int kThreads = 192;     // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int kMaxStages = 32;
 constexpr int kConvM = 128;       // pixels per convolution tile = TMEM lanes
-constexpr int kWgK = 64;          // pixels per weight-gradient stage
+constexpr int kWgK = 128;         // pixels per weight-gradient stage
 constexpr uint32_t kOnesBytes = 1024;
 
 __device__ int g_nn_tma_err;
@@ -292,7 +294,7 @@ struct WgradArgs {
     int bw, tiles_x, tiles_y, ntiles, tiles_per_chunk;
     int cbo, swo, nbo;  // dout channel blocks: channels, row bytes, count
     int cbi, swi, nbi;  // input channel blocks
-    int tpg;            // taps per group
+    int tpg, tps;       // taps per group (grid y); taps per MMA (tps x Cin <= 256)
     int stages;
     uint32_t stage_bytes, a_bytes, b_bytes;  // b_bytes: one tap's input box
     uint32_t a_lbo;                          // 0 when one block holds every output channel
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t id_w = idesc(128, a.Cin, true, true), id_b = idesc(128, 16, true, true);
+            const uint32_t id_b = idesc(128, 16, true, true);
             const uint32_t la = layout_of(a.swo), lb = layout_of(a.swi);
             const uint32_t sbo_a = 8u * (uint32_t)a.swo, sbo_b = 8u * (uint32_t)a.swi;
             const uint32_t lbo_b = (uint32_t)kWgK * (uint32_t)a.swi;
@@ -395,10 +397,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                     // K step: 16 pixels = two 8-row groups of each operand
                     const uint64_t da = mdesc(sa + 16u * k * (uint32_t)a.swo, a.a_lbo, sbo_a, la);
                     const bool acc = (it | (uint32_t)k) != 0;
-                    for (int j = 0; j < ntap; ++j)
+                    // the taps' input blocks are b_bytes = nbi x kWgK x swi apart, i.e. every
+                    // cbi-channel block of the group sits lbo_b after the previous one: up to tps
+                    // taps form one MMA with N = taps x Cin
+                    for (int j = 0; j < ntap; j += a.tps) {
+                        const int nt = ntap - j < a.tps ? ntap - j : a.tps;
                         mma(tmem + (uint32_t)(j * a.Cin), da,
-                            mdesc(sb + (uint32_t)j * a.b_bytes + 16u * k * (uint32_t)a.swi, lbo_b, sbo_b, lb), id_w,
-                            acc);
+                            mdesc(sb + (uint32_t)j * a.b_bytes + 16u * k * (uint32_t)a.swi, lbo_b, sbo_b, lb),
+                            idesc(128, nt * a.Cin, true, true), acc);
+                    }
                     if (with_bias) mma(tmem + (uint32_t)(ntap * a.Cin), da, d_ones, id_b, acc);
                 }
                 commit(&empty[s]);
@@ -440,6 +447,202 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ------------------------------------------------------------ halo kernels
+// A tile is 8 pixels wide and 16 rows tall (128 pixels).  Its input plus a
+// one-pixel border (10 x 18 pixels) comes in once per tile, one 4-D TMA box
+// per 8-channel plane, in the canonical no-swizzle layout: plane j holds
+// [18 rows][10 pixels][8 channels], 16 bytes a pixel.  Every tap reads the
+// same planes from a shifted start: the 8 pixels of a tile row are one core
+// matrix, tile rows are one halo row (160 B) apart, planes kHaloPlane apart.
+// Nine taps thus cost one load per plane instead of nine, and no MMA row is
+// wasted (8-pixel tile rows never wrap inside a core matrix).
+constexpr int kHx = 8, kHy = 16;
+constexpr int kHaloW = kHx + 2, kHaloH = kHy + 2;
+constexpr uint32_t kHaloBox = kHaloW * kHaloH * 16;  // 2880 B
+constexpr uint32_t kHaloPlane = 2944;                // the box rounded up to 128 B
+constexpr uint32_t kHaloRow = kHaloW * 16;           // 160 B
+
+__device__ __forceinline__ void halo_tile_origin(int tiles_x, int tiles_y, int t, int& n, int& x0, int& y0) {
+    const int tx = t % tiles_x;
+    const int r = t / tiles_x;
+    x0 = tx * kHx;
+    y0 = (r % tiles_y) * kHy;
+    n = r / tiles_y;
+}
+
+// shared-memory offset of tap `tap`'s first pixel in a halo plane
+__device__ __forceinline__ uint32_t tap_offset(int tap) { return (uint32_t)((tap / 3) * kHaloW + tap % 3) * 16u; }
+
+struct HaloConvArgs {
+    int H, W, Cin, Cout;
+    int tiles_x, tiles_y, ntiles;
+    int planes;  // Cin / 8
+    int stages;
+    uint32_t stage_bytes, w_bytes;  // one tile's planes; the resident weights (rounded to 1024)
+    int ncols;
+    const __nv_bfloat16* w;  // [Cout][9][Cin]
+    const float* bias;
+    int relu;
+    __nv_bfloat16* out;
+    float* out32;
+};
+
+// Convolution with the weights resident in shared memory: [tap][ci / 8][co][8]
+// (K-major B: core matrices of 8 output channels x 16 B, 128 B apart; the
+// next 8 input channels Cout x 16 B further).
+__global__ void __launch_bounds__(kThreads, 1)
+    conv3x3_halo_kernel(const __grid_constant__ CUtensorMap m_in, const HaloConvArgs a) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = align1024(smem_raw);
+    unsigned char* ring = smem + a.w_bytes;
+    __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], tfull[2], tempty[2], fin;
+    __shared__ uint32_t tmem_slot;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kc = a.Cin / 8;
+
+    for (int e = threadIdx.x; e < 9 * kc * a.Cout; e += kThreads) {
+        const int co = e % a.Cout, r = e / a.Cout;
+        const int j = r % kc, tap = r / kc;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.w + ((size_t)co * 9 + tap) * a.Cin + 8 * j));
+        *reinterpret_cast<uint4*>(smem + ((size_t)r * a.Cout + co) * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tensor cores read them
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, a.ncols);
+        fence_before();
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.stages; ++s) {
+            tma::mbar_init(&full[s], 1);
+            tma::mbar_init(&empty[s], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            tma::mbar_init(&tfull[i], 1);
+            tma::mbar_init(&tempty[i], 4);
+        }
+        tma::mbar_init(&fin, 1);
+        tma::fence_barrier_init();
+        tma::prefetch_map(&m_in);
+    }
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint32_t tx = (uint32_t)a.planes * kHaloBox;
+            int s = 0;
+            uint32_t ph = 0, used = 0;
+            for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+                if (!tma::mbar_wait(&empty[s], ph ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                int n, x0, y0;
+                halo_tile_origin(a.tiles_x, a.tiles_y, t, n, x0, y0);
+                unsigned char* st = ring + (size_t)s * a.stage_bytes;
+                tma::mbar_arrive_expect_tx(&full[s], tx);
+                for (int j = 0; j < a.planes; ++j)
+                    tma::load_4d(st + (size_t)j * kHaloPlane, &m_in, 8 * j, x0 - 1, y0 - 1, n, &full[s]);
+                ++used;
+                if (++s == a.stages) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            // the last fill of every stage has landed before the CTA can exit
+            for (int q = 0; q < a.stages; ++q)
+                if ((uint32_t)q < used && !tma::mbar_wait(&full[q], ((used - 1 - q) / (uint32_t)a.stages) & 1u))
+                    ok = false;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t id = idesc(kConvM, a.Cout, false, false);
+            const uint32_t wb = saddr(smem), wstep = (uint32_t)a.Cout * 16u;
+            int s = 0, local = 0;
+            uint32_t ph = 0;
+            for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++local) {
+                const int acc = local & 1;
+                if (!tma::mbar_wait(&tempty[acc], (((uint32_t)local >> 1) & 1u) ^ 1u) ||
+                    !tma::mbar_wait(&full[s], ph)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t d = tmem + (uint32_t)(acc * a.Cout);
+                const uint32_t hb = saddr(ring + (size_t)s * a.stage_bytes);
+                for (int tap = 0; tap < 9; ++tap) {
+                    const uint64_t da0 = mdesc(hb + tap_offset(tap), kHaloPlane, kHaloRow, 0u);
+                    const uint64_t db0 = mdesc(wb + (uint32_t)(tap * kc) * wstep, wstep, 128u, 0u);
+                    for (int k = 0; k < kc / 2; ++k)
+                        // K step k: planes 2k, 2k + 1 (start addresses advance in 16-B units)
+                        mma(d, da0 + (uint64_t)((2u * k * kHaloPlane) >> 4), db0 + (uint64_t)((2u * k * wstep) >> 4),
+                            id, (tap | k) != 0);
+                }
+                commit(&empty[s]);
+                commit(&tfull[acc]);
+                if (++s == a.stages) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            commit(&fin);
+            if (!tma::mbar_wait(&fin, 0u)) ok = false;
+        }
+    } else {
+        const int q = warp & 3;
+        const int m = q * 32 + lane;
+        int local = 0;
+        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++local) {
+            const int acc = local & 1;
+            if (!tma::mbar_wait(&tfull[acc], ((uint32_t)local >> 1) & 1u)) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            int n, x0, y0;
+            halo_tile_origin(a.tiles_x, a.tiles_y, t, n, x0, y0);
+            const int yy = y0 + m / kHx, xx = x0 + m % kHx;
+            const bool valid = yy < a.H && xx < a.W;
+            const long long p = ((long long)n * a.H + yy) * a.W + xx;
+            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * a.Cout);
+            for (int c0 = 0; c0 < a.Cout; c0 += 8) {
+                uint32_t r[8];
+                tmem_ld8(base + (uint32_t)c0, r);
+                if (!valid) continue;
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float x = __uint_as_float(r[j]);
+                    if (a.bias) x += __ldg(a.bias + c0 + j);
+                    if (a.relu) x = fmaxf(x, 0.0f);
+                    v[j] = x;
+                }
+                if (a.out)
+                    *reinterpret_cast<uint4*>(a.out + p * a.Cout + c0) =
+                        make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                   pack_bf16x2(v[6], v[7]));
+                if (a.out32) {
+                    float4* o = reinterpret_cast<float4*>(a.out32 + p * a.Cout + c0);
+                    o[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    o[1] = make_float4(v[4], v[5], v[6], v[7]);
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) tma::mbar_arrive(&tempty[acc]);
+        }
+    }
+    if (!ok) atomicExch(&g_nn_tma_err, 1);
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        tmem_free(tmem, a.ncols);
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------- host
@@ -469,8 +672,10 @@ CUtensorMapSwizzle swizzle_of(int row_bytes) {
                             : row_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
 }
 
-// NHWC bf16 activations as the 4-D tensor (C, W, H, N), box (cb, bw, bh, 1).
-bool act_map(CUtensorMap* m, const void* base, int N, int H, int W, int C, int cb, int bw, int bh) {
+// NHWC bf16 activations as the 4-D tensor (C, W, H, N), box (cb, bw, bh, 1);
+// rows of 2 cb bytes swizzled to match (cb = 64, 32, 16), or not swizzled.
+bool act_map(CUtensorMap* m, const void* base, int N, int H, int W, int C, int cb, int bw, int bh,
+             bool swizzled = true) {
     auto enc = encoder();
     if (!enc) return false;
     cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
@@ -478,8 +683,8 @@ bool act_map(CUtensorMap* m, const void* base, int N, int H, int W, int C, int c
     cuuint32_t box[4] = {(cuuint32_t)cb, (cuuint32_t)bw, (cuuint32_t)bh, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(2 * cb), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzled ? swizzle_of(2 * cb) : CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Weights [Cout][9][Cin] as the 3-D tensor (Cin, 9, Cout), box (cb, 1, Cout).
@@ -540,6 +745,8 @@ size_t max_dynamic_smem(K kernel) {
     return cap;
 }
 
+constexpr uint32_t kStageCap = 72 * 1024;  // weight-gradient stage bound
+
 struct WgPlan {
     WgradArgs a;
     int chunks, ngroups, bh;
@@ -559,11 +766,18 @@ bool wg_plan(int N, int H, int W, int Cin, int Cout, size_t smem_cap, WgPlan& p)
     a.cbi = channel_block(Cin);
     a.swi = 2 * a.cbi;
     a.nbi = Cin / a.cbi;
-    // every tap of a group has Cin TMEM columns, the bias 16 more
+    // every tap of a group has Cin TMEM columns, the bias 16 more; a stage
+    // (output-gradient box + one input box per tap) stays within kStageCap
+    a.a_bytes = a.nbo == 1 ? (uint32_t)kWgK * a.swo : 128u * kWgK * 2u;
+    a.b_bytes = (uint32_t)kWgK * Cin * 2u;
     int tpg = (512 - 16) / Cin;
+    int by_smem = a.a_bytes < kStageCap ? (int)((kStageCap - a.a_bytes) / a.b_bytes) : 0;
+    if (by_smem < 1) by_smem = 1;
+    if (tpg > by_smem) tpg = by_smem;
     if (tpg > 9) tpg = 9;
     p.ngroups = (9 + tpg - 1) / tpg;
     a.tpg = (9 + p.ngroups - 1) / p.ngroups;
+    a.tps = 256 / Cin < a.tpg ? 256 / Cin : a.tpg;
     a.bw = box_width(H, W, kWgK);
     p.bh = kWgK / a.bw;
     a.tiles_x = (W + a.bw - 1) / a.bw;
@@ -579,9 +793,7 @@ bool wg_plan(int N, int H, int W, int Cin, int Cout, size_t smem_cap, WgPlan& p)
     // one dout block covering every output channel: the MMA's 128 rows all
     // read it (rows past Cout are never stored); else the blocks sit kWgK * swo
     // apart in a region of 128 rows
-    a.a_bytes = a.nbo == 1 ? (uint32_t)kWgK * a.swo : 128u * kWgK * 2u;
     a.a_lbo = a.nbo == 1 ? 0u : (uint32_t)kWgK * a.swo;
-    a.b_bytes = (uint32_t)kWgK * Cin * 2u;
     a.stage_bytes = a.a_bytes + (uint32_t)a.tpg * a.b_bytes;
     const size_t budget = smem_cap > 1024 + kOnesBytes ? smem_cap - 1024 - kOnesBytes : 0;
     size_t st = budget / a.stage_bytes;
@@ -592,12 +804,55 @@ bool wg_plan(int N, int H, int W, int Cin, int Cout, size_t smem_cap, WgPlan& p)
     return a.ncols <= 512;
 }
 
+// Convolution over 8 x 16 tiles with resident weights: taken when the
+// weights and two halo stages fit in shared memory, and either the weights are
+// small or every CTA has at least two tiles to spread their load over.
+bool halo_conv_plan(int N, int H, int W, int Cin, int Cout, size_t cap, HaloConvArgs& h) {
+    h = HaloConvArgs{};
+    h.H = H;
+    h.W = W;
+    h.Cin = Cin;
+    h.Cout = Cout;
+    h.tiles_x = (W + kHx - 1) / kHx;
+    h.tiles_y = (H + kHy - 1) / kHy;
+    const long long nt = (long long)N * h.tiles_x * h.tiles_y;
+    if (nt > (1LL << 30)) return false;
+    h.ntiles = (int)nt;
+    h.planes = Cin / 8;
+    h.stage_bytes = ((uint32_t)h.planes * kHaloPlane + 1023u) / 1024u * 1024u;
+    h.w_bytes = ((uint32_t)(9 * Cin * Cout * 2) + 1023u) / 1024u * 1024u;
+    if (h.w_bytes > 40 * 1024 && h.ntiles < 2 * kSmTarget) return false;
+    if (cap < 1024 + (size_t)h.w_bytes + 2 * (size_t)h.stage_bytes) return false;
+    size_t st = (cap - 1024 - h.w_bytes) / h.stage_bytes;
+    if (st > (size_t)kMaxStages) st = kMaxStages;
+    h.stages = (int)st;
+    h.ncols = tmem_columns(2 * Cout);
+    return true;
+}
+
 }  // namespace
 
 int nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, const float* bias, int Cout, int relu,
                    void* out, float* out32, cudaStream_t st) {
     if (Cin % 16 || Cin > 256 || Cout % 16 || Cout > 256 || N < 1 || H < 1 || W < 1) return -1;
     if (!aligned16(in) || !aligned16(w) || !aligned16(out) || !aligned16(out32)) return -1;
+    static size_t hcap = 0;
+    if (hcap == 0 && (hcap = max_dynamic_smem(conv3x3_halo_kernel)) == 0) return -2;
+    HaloConvArgs h;
+    if (halo_conv_plan(N, H, W, Cin, Cout, hcap, h)) {
+        h.w = static_cast<const __nv_bfloat16*>(w);
+        h.bias = bias;
+        h.relu = relu;
+        h.out = static_cast<__nv_bfloat16*>(out);
+        h.out32 = out32;
+        CUtensorMap mh;
+        if (!act_map(&mh, in, N, H, W, Cin, 8, kHaloW, kHaloH, false)) return -2;
+        size_t dyn = 1024 + (size_t)h.w_bytes + (size_t)h.stages * h.stage_bytes;
+        if (dyn < kOneCtaPerSm) dyn = kOneCtaPerSm;
+        const int grid = h.ntiles < sm_count() ? h.ntiles : sm_count();
+        conv3x3_halo_kernel<<<grid, kThreads, dyn, st>>>(mh, h);
+        return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    }
     static size_t cap = 0;
     if (cap == 0 && (cap = max_dynamic_smem(conv3x3_tma_kernel)) == 0) return -2;
     ConvArgs a{};

@@ -43,9 +43,10 @@ int fwi_nn_check(void);
 size_t fwi_nn_wgrad_partial_floats(int N, int H, int W, int Cin, int Cout);
 int fwi_nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
                          float* dw, float* db, void* stream);
-/* The per-chunk sums run on the tcgen05 tensor cores (M = output channels
- * padded to 128, N = input channels, K = pixels, both operands MN-major) for
- * Cout <= 128, else on mma.sync; _mma always uses mma.sync (for comparison). */
+/* The per-chunk sums run on the tcgen05 tensor cores for Cout <= 128 (M =
+ * output channels padded to 128, N = several taps x input channels, K =
+ * pixels, both operands MN-major; the bias gradient as one more MMA against
+ * ones), else on mma.sync; _mma always uses mma.sync (for comparison). */
 int fwi_nn_conv3x3_wgrad_mma(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial,
                              float* dw, float* db, void* stream);
 /* bf16 copy of float32 weights w and (wt != NULL) the data-gradient weights
