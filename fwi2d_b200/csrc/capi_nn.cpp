@@ -1,5 +1,6 @@
 // capi_nn.cpp — extern "C" surface of fwi2d_nn.h over the kernels of k_nn.cu.
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "../../include/fwi2d.h"
 #include "../../include/fwi2d_nn.h"
@@ -9,6 +10,8 @@ namespace {
 cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 int status() { return cudaGetLastError() == cudaSuccess ? FWI_OK : FWI_ERR_CUDA; }
 bool dims_ok(int N, int H, int W) { return N >= 1 && H >= 1 && W >= 1; }
+// the element-wise kernels move 8 channels (16 or 32 bytes) at a time
+bool vec_ok(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 }  // namespace
 
 extern "C" {
@@ -69,40 +72,46 @@ int fwi_nn_weight_prep(const float* w, int Cout, int Cin, void* w_bf16, void* wt
 }
 
 int fwi_nn_pool2(const void* in, int N, int H, int W, int C, void* out, void* stream) {
-    if (!in || !out || !dims_ok(N, H / 2, W / 2) || C < 1) return FWI_ERR_ARG;
+    if (!in || !out || !dims_ok(N, H / 2, W / 2) || C < 1 || C % 8 || !vec_ok(in) || !vec_ok(out)) return FWI_ERR_ARG;
     fwi::nn_pool_fwd(in, N, H, W, C, out, S(stream));
     return status();
 }
 
 int fwi_nn_pool2_bwd(const float* dout, int N, int H, int W, int C, float* din, int accumulate, void* stream) {
-    if (!dout || !din || !dims_ok(N, H / 2, W / 2) || C < 1) return FWI_ERR_ARG;
+    if (!dout || !din || !dims_ok(N, H / 2, W / 2) || C < 1 || C % 8 || !vec_ok(dout) || !vec_ok(din))
+        return FWI_ERR_ARG;
     fwi::nn_pool_bwd(dout, N, H, W, C, din, accumulate, S(stream));
     return status();
 }
 
 int fwi_nn_upcat(const void* a, int Hs, int Ws, int C1, const void* skip, int N, int H, int W, int C2, void* out,
                  void* stream) {
-    if (!a || !skip || !out || !dims_ok(N, H, W) || Hs < 1 || Ws < 1 || C1 < 1 || C2 < 1) return FWI_ERR_ARG;
+    if (!a || !skip || !out || !dims_ok(N, H, W) || Hs < 1 || Ws < 1 || C1 < 1 || C2 < 1 || C1 % 8 || C2 % 8 ||
+        !vec_ok(a) || !vec_ok(skip) || !vec_ok(out))
+        return FWI_ERR_ARG;
     fwi::nn_upcat_fwd(a, Hs, Ws, C1, skip, N, H, W, C2, out, S(stream));
     return status();
 }
 
 int fwi_nn_upcat_bwd(const float* dout, int N, int H, int W, int C1, int C2, int Hs, int Ws, float* da, int acc_a,
                      float* dskip, int acc_skip, void* stream) {
-    if (!dout || !da || !dskip || !dims_ok(N, H, W) || Hs < 1 || Ws < 1) return FWI_ERR_ARG;
+    if (!dout || !da || !dskip || !dims_ok(N, H, W) || Hs < 1 || Ws < 1 || C1 < 8 || C2 < 8 || C1 % 8 || C2 % 8 ||
+        !vec_ok(dout) || !vec_ok(da) || !vec_ok(dskip))
+        return FWI_ERR_ARG;
     fwi::nn_upcat_bwd(dout, N, H, W, C1, C2, Hs, Ws, da, acc_a, dskip, acc_skip, S(stream));
     return status();
 }
 
 int fwi_nn_relu_bwd(const float* da, const void* a, size_t n, void* dpre, void* stream) {
-    if (!da || !a || !dpre) return FWI_ERR_ARG;
+    if (!da || !a || !dpre || n % 8 || !vec_ok(da) || !vec_ok(a) || !vec_ok(dpre)) return FWI_ERR_ARG;
     fwi::nn_relu_bwd(da, a, n, dpre, S(stream));
     return status();
 }
 
 int fwi_nn_mse(const float* out_f32, int C, const float* target, const float* mask, long long P, float scale,
                void* dout, double* partial, double* loss, void* stream) {
-    if (!out_f32 || !target || !dout || !partial || !loss || C < 1 || P < 1) return FWI_ERR_ARG;
+    if (!out_f32 || !target || !dout || !partial || !loss || C < 8 || C % 8 || P < 1 || !vec_ok(dout))
+        return FWI_ERR_ARG;
     fwi::nn_mse(out_f32, C, target, mask, P, scale, dout, partial, loss, S(stream));
     return status();
 }

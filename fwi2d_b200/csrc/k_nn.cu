@@ -2,8 +2,12 @@
 // the FWI gradient, illumination and model; no reference counterpart).
 //
 // Activations are NHWC bfloat16 (channels innermost, a multiple of 16);
-// gradients of activations are float32.  Every 3x3 convolution is an implicit
-// GEMM on the BF16 tensor cores with FP32 accumulation (mma.sync m16n8k16):
+// gradients of activations are float32.  The convolutions the network runs
+// are the tcgen05 kernels of k_nn_tma.cu; this file holds the element-wise
+// layers, the fixed-order reductions, Adam, and the first implementation of
+// the convolutions on the warp-level tensor-core path (mma.sync m16n8k16,
+// fwi_nn_conv3x3_mma / _wgrad_mma, kept for comparison), implicit GEMMs with
+// FP32 accumulation:
 //   forward   out[p, co] = sum_{tap, ci} in[p + tap, ci] * w[co, tap, ci]
 //   data grad the same kernel on the output gradient with the flipped,
 //             transposed weights wT[ci, 8 - tap, co]
@@ -174,14 +178,43 @@ __global__ void __launch_bounds__(32 * kWarps) wgrad_kernel(const __nv_bfloat16*
     }
 }
 
-// dW = sum of the chunk partials in chunk order; db[co] = sum over pixels of dout
-__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int chunks, size_t nw, float* __restrict__ dw) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nw; i += (size_t)gridDim.x * blockDim.x) {
-        float s = 0.0f;
-        for (int c = 0; c < chunks; ++c) s += partial[(size_t)c * nw + i];
-        dw[i] = s;
+// dW = sum of the chunk partials, in a fixed order: thread (column, slice)
+// sums four consecutive outputs over the chunks slice, slice + 8, ... and the
+// eight slices are then added in slice order.  nw is a multiple of 4.
+constexpr int kSlices = 8;
+
+__global__ void __launch_bounds__(32 * kSlices) wgrad_reduce_kernel(const float* __restrict__ partial, int chunks,
+                                                                    size_t nw, float* __restrict__ dw) {
+    __shared__ float4 red[kSlices][32];
+    const int col = threadIdx.x & 31, slice = threadIdx.x >> 5;
+    const size_t i = ((size_t)blockIdx.x * 32 + col) * 4;
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (i < nw) {
+#pragma unroll 4
+        for (int c = slice; c < chunks; c += kSlices) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(partial + (size_t)c * nw + i));
+            s.x += v.x;
+            s.y += v.y;
+            s.z += v.z;
+            s.w += v.w;
+        }
+    }
+    red[slice][col] = s;
+    __syncthreads();
+    if (slice == 0 && i < nw) {
+        float4 t = red[0][col];
+        for (int q = 1; q < kSlices; ++q) {
+            const float4 v = red[q][col];
+            t.x += v.x;
+            t.y += v.y;
+            t.z += v.z;
+            t.w += v.w;
+        }
+        *reinterpret_cast<float4*>(dw + i) = t;
     }
 }
+
+unsigned reduce_blocks(size_t nw) { return (unsigned)((nw / 4 + 31) / 32); }
 
 __global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dout, long long P, int Cout, float* __restrict__ db) {
     // one CTA per output channel, fixed-order tree in shared memory
@@ -234,34 +267,81 @@ __global__ void weight_prep_kernel(const float* __restrict__ w, int Cout, int Ci
     }
 }
 
+// The element-wise kernels below move 8 channels (16 B of bf16, 32 B of
+// float32) per thread; every channel count is a multiple of 8.
+__device__ __forceinline__ void unpack8(const uint4 v, float f[8]) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        f[2 * k] = __uint_as_float(w[k] << 16);
+        f[2 * k + 1] = __uint_as_float(w[k] & 0xFFFF0000u);
+    }
+}
+
+__device__ __forceinline__ uint4 pack8(const float f[8]) {
+    uint32_t w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        w[k] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f[2 * k])) |
+               ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f[2 * k + 1])) << 16);
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ void load8(const float* p, float f[8]) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p + 4));
+    f[0] = a.x, f[1] = a.y, f[2] = a.z, f[3] = a.w, f[4] = b.x, f[5] = b.y, f[6] = b.z, f[7] = b.w;
+}
+
+__device__ __forceinline__ void store8(float* p, const float f[8]) {
+    reinterpret_cast<float4*>(p)[0] = make_float4(f[0], f[1], f[2], f[3]);
+    reinterpret_cast<float4*>(p)[1] = make_float4(f[4], f[5], f[6], f[7]);
+}
+
 // 2x2 average pooling (floor sizes), NHWC bf16 -> bf16
 __global__ void pool_fwd_kernel(const __nv_bfloat16* __restrict__ in, int N, int H, int W, int C,
                                 __nv_bfloat16* __restrict__ out) {
-    const int Ho = H / 2, Wo = W / 2;
-    const size_t n = (size_t)N * Ho * Wo * C;
+    const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+    const size_t n = (size_t)N * Ho * Wo * C8;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t q = i / C;
+        const int c = (int)(i % C8) * 8;
+        const size_t q = i / C8;
         const int x = (int)(q % Wo), y = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
         const size_t r0 = (((size_t)b * H + 2 * y) * W + 2 * x) * C + c;
-        const float s = (__bfloat162float(in[r0]) + __bfloat162float(in[r0 + C])) +
-                        (__bfloat162float(in[r0 + (size_t)W * C]) + __bfloat162float(in[r0 + (size_t)W * C + C]));
-        out[i] = __float2bfloat16_rn(0.25f * s);
+        float p00[8], p01[8], p10[8], p11[8], o[8];
+        unpack8(__ldg(reinterpret_cast<const uint4*>(in + r0)), p00);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(in + r0 + C)), p01);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(in + r0 + (size_t)W * C)), p10);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(in + r0 + (size_t)W * C + C)), p11);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o[k] = 0.25f * ((p00[k] + p01[k]) + (p10[k] + p11[k]));
+        *reinterpret_cast<uint4*>(out + q * C + c) = pack8(o);
     }
 }
 
 // gradient of the pooling: din (+)= dout / 4 on the pooled pixels, 0 on the dropped edge
 __global__ void pool_bwd_kernel(const float* __restrict__ dout, int N, int H, int W, int C, float* __restrict__ din,
                                 int accumulate) {
-    const int Ho = H / 2, Wo = W / 2;
-    const size_t n = (size_t)N * H * W * C;
+    const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+    const size_t n = (size_t)N * H * W * C8;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t q = i / C;
+        const int c = (int)(i % C8) * 8;
+        const size_t q = i / C8;
         const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
         const int xo = x / 2, yo = y / 2;
-        const float g = (xo < Wo && yo < Ho) ? 0.25f * dout[(((size_t)b * Ho + yo) * Wo + xo) * C + c] : 0.0f;
-        din[i] = accumulate ? din[i] + g : g;
+        float g[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (xo < Wo && yo < Ho) {
+            load8(dout + (((size_t)b * Ho + yo) * Wo + xo) * C + c, g);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) g[k] *= 0.25f;
+        }
+        float* d = din + q * C + c;
+        if (accumulate) {
+            float o[8];
+            load8(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) g[k] += o[k];
+        }
+        store8(d, g);
     }
 }
 
@@ -270,18 +350,20 @@ __global__ void pool_bwd_kernel(const float* __restrict__ dout, int N, int H, in
 __global__ void upcat_fwd_kernel(const __nv_bfloat16* __restrict__ a, int Hs, int Ws, int C1,
                                  const __nv_bfloat16* __restrict__ skip, int N, int H, int W, int C2,
                                  __nv_bfloat16* __restrict__ out) {
-    const int C = C1 + C2;
-    const size_t n = (size_t)N * H * W * C;
+    const int C8 = (C1 + C2) / 8;
+    const size_t n = (size_t)N * H * W * C8;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t q = i / C;
+        const int c = (int)(i % C8) * 8;
+        const size_t q = i / C8;
         const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
+        uint4 v;
         if (c < C1) {
             const int ys = min(y / 2, Hs - 1), xs = min(x / 2, Ws - 1);
-            out[i] = a[(((size_t)b * Hs + ys) * Ws + xs) * C1 + c];
+            v = __ldg(reinterpret_cast<const uint4*>(a + (((size_t)b * Hs + ys) * Ws + xs) * C1 + c));
         } else {
-            out[i] = skip[q * C2 + (c - C1)];
+            v = __ldg(reinterpret_cast<const uint4*>(skip + q * C2 + (c - C1)));
         }
+        reinterpret_cast<uint4*>(out)[i] = v;
     }
 }
 
@@ -289,36 +371,64 @@ __global__ void upcat_fwd_kernel(const __nv_bfloat16* __restrict__ a, int Hs, in
 // dskip += dout[..., C1:]
 __global__ void upcat_bwd_a_kernel(const float* __restrict__ dout, int N, int H, int W, int C1, int C2, int Hs,
                                    int Ws, float* __restrict__ da, int accumulate) {
-    const int C = C1 + C2;
-    const size_t n = (size_t)N * Hs * Ws * C1;
+    const int C = C1 + C2, C8 = C1 / 8;
+    const size_t n = (size_t)N * Hs * Ws * C8;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C1);
-        const size_t q = i / C1;
+        const int c = (int)(i % C8) * 8;
+        const size_t q = i / C8;
         const int xs = (int)(q % Ws), ys = (int)((q / Ws) % Hs), b = (int)(q / ((size_t)Ws * Hs));
         const int ya = 2 * ys, yb = (ys == Hs - 1) ? H : min(2 * ys + 2, H);
         const int xa = 2 * xs, xb = (xs == Ws - 1) ? W : min(2 * xs + 2, W);
-        float s = 0.0f;
+        float s[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         for (int y = ya; y < yb; ++y)
-            for (int x = xa; x < xb; ++x) s += dout[(((size_t)b * H + y) * W + x) * C + c];
-        da[i] = accumulate ? da[i] + s : s;
+            for (int x = xa; x < xb; ++x) {
+                float g[8];
+                load8(dout + (((size_t)b * H + y) * W + x) * C + c, g);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) s[k] += g[k];
+            }
+        float* d = da + q * C1 + c;
+        if (accumulate) {
+            float o[8];
+            load8(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s[k] = o[k] + s[k];
+        }
+        store8(d, s);
     }
 }
 
 __global__ void upcat_bwd_skip_kernel(const float* __restrict__ dout, size_t npix, int C1, int C2,
                                       float* __restrict__ dskip, int accumulate) {
-    const size_t n = npix * C2;
+    const int C8 = C2 / 8;
+    const size_t n = npix * C8;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const size_t p = i / C2;
-        const float g = dout[p * (C1 + C2) + C1 + (i % C2)];
-        dskip[i] = accumulate ? dskip[i] + g : g;
+        const size_t p = i / C8;
+        const int c = (int)(i % C8) * 8;
+        float g[8];
+        load8(dout + p * (C1 + C2) + C1 + c, g);
+        float* d = dskip + p * C2 + c;
+        if (accumulate) {
+            float o[8];
+            load8(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) g[k] = o[k] + g[k];
+        }
+        store8(d, g);
     }
 }
 
-// dpre = da * (a > 0) as bf16 (the ReLU gradient, a the stored activation)
+// dpre = da * (a > 0) as bf16 (the ReLU gradient, a the stored activation); n a multiple of 8
 __global__ void relu_bwd_kernel(const float* __restrict__ da, const __nv_bfloat16* __restrict__ a, size_t n,
                                 __nv_bfloat16* __restrict__ dpre) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        dpre[i] = __float2bfloat16_rn(__bfloat162float(a[i]) > 0.0f ? da[i] : 0.0f);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n / 8; i += (size_t)gridDim.x * blockDim.x) {
+        float g[8], v[8];
+        load8(da + 8 * i, g);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(a) + i), v);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) g[k] = v[k] > 0.0f ? g[k] : 0.0f;
+        reinterpret_cast<uint4*>(dpre)[i] = pack8(g);
+    }
 }
 
 // Mean-squared error of channel 0 of out32 ([P, C]) against target [P] on the
@@ -333,8 +443,9 @@ __global__ void mse_kernel(const float* __restrict__ out32, int C, const float* 
         const float m = mask ? mask[p] : 1.0f;
         const float d = (out32[p * C] - target[p]) * m;
         s += (double)d * (double)d;
-        dout[p * C] = __float2bfloat16_rn(2.0f * d * scale);
-        for (int c = 1; c < C; ++c) dout[p * C + c] = __float2bfloat16_rn(0.0f);
+        uint4* o = reinterpret_cast<uint4*>(dout + p * C);  // C a multiple of 8
+        o[0] = make_uint4((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(2.0f * d * scale)), 0u, 0u, 0u);
+        for (int c = 1; c < C / 8; ++c) o[c] = make_uint4(0u, 0u, 0u, 0u);
     }
     red[threadIdx.x] = s;
     __syncthreads();
@@ -461,9 +572,9 @@ int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int 
         const int tc_chunks = nn_wgrad_tma(in, dout, N, H, W, Cin, Cout, partial, db != nullptr, st);
         if (tc_chunks == -2) return -2;
         if (tc_chunks > 0) {
-            wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, tc_chunks, nw, dw);
+            wgrad_reduce_kernel<<<reduce_blocks(nw), 32 * kSlices, 0, st>>>(partial, tc_chunks, nw, dw);
             if (db)
-                wgrad_reduce_kernel<<<grid_n((size_t)Cout), 256, 0, st>>>(partial + (size_t)tc_chunks * nw, tc_chunks,
+                wgrad_reduce_kernel<<<reduce_blocks((size_t)Cout), 32 * kSlices, 0, st>>>(partial + (size_t)tc_chunks * nw, tc_chunks,
                                                                           (size_t)Cout, db);
             return 0;
         }
@@ -475,11 +586,11 @@ int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int 
         dim3 grid(chunks, 9, (Cout / 16) * (Cin / 16));
         wgrad_kernel<2><<<grid, 32 * kWarps, 0, st>>>(i16, d16, N, H, W, Cin, Cout, chunk, partial);
     }
-    wgrad_reduce_kernel<<<grid_n(nw), 256, 0, st>>>(partial, chunks, nw, dw);
+    wgrad_reduce_kernel<<<reduce_blocks(nw), 32 * kSlices, 0, st>>>(partial, chunks, nw, dw);
     if (db) {
         if (256 % Cout == 0) {  // the chunk partials are consumed: reuse the scratch
             bias_partial_kernel<<<chunks, 256, 0, st>>>(d16, P, Cout, chunk, partial);
-            wgrad_reduce_kernel<<<grid_n((size_t)Cout), 256, 0, st>>>(partial, chunks, (size_t)Cout, db);
+            wgrad_reduce_kernel<<<reduce_blocks((size_t)Cout), 32 * kSlices, 0, st>>>(partial, chunks, (size_t)Cout, db);
         } else {
             bias_grad_kernel<<<Cout, 256, 0, st>>>(d16, P, Cout, db);
         }
@@ -494,30 +605,30 @@ void nn_weight_prep(const float* w, int Cout, int Cin, void* wb, void* wt, cudaS
 }
 
 void nn_pool_fwd(const void* in, int N, int H, int W, int C, void* out, cudaStream_t st) {
-    pool_fwd_kernel<<<grid_n((size_t)N * (H / 2) * (W / 2) * C), 256, 0, st>>>(
+    pool_fwd_kernel<<<grid_n((size_t)N * (H / 2) * (W / 2) * C / 8), 256, 0, st>>>(
         static_cast<const __nv_bfloat16*>(in), N, H, W, C, static_cast<__nv_bfloat16*>(out));
 }
 
 void nn_pool_bwd(const float* dout, int N, int H, int W, int C, float* din, int accumulate, cudaStream_t st) {
-    pool_bwd_kernel<<<grid_n((size_t)N * H * W * C), 256, 0, st>>>(dout, N, H, W, C, din, accumulate);
+    pool_bwd_kernel<<<grid_n((size_t)N * H * W * C / 8), 256, 0, st>>>(dout, N, H, W, C, din, accumulate);
 }
 
 void nn_upcat_fwd(const void* a, int Hs, int Ws, int C1, const void* skip, int N, int H, int W, int C2, void* out,
                   cudaStream_t st) {
-    upcat_fwd_kernel<<<grid_n((size_t)N * H * W * (C1 + C2)), 256, 0, st>>>(
+    upcat_fwd_kernel<<<grid_n((size_t)N * H * W * (C1 + C2) / 8), 256, 0, st>>>(
         static_cast<const __nv_bfloat16*>(a), Hs, Ws, C1, static_cast<const __nv_bfloat16*>(skip), N, H, W, C2,
         static_cast<__nv_bfloat16*>(out));
 }
 
 void nn_upcat_bwd(const float* dout, int N, int H, int W, int C1, int C2, int Hs, int Ws, float* da, int acc_a,
                   float* dskip, int acc_skip, cudaStream_t st) {
-    upcat_bwd_a_kernel<<<grid_n((size_t)N * Hs * Ws * C1), 256, 0, st>>>(dout, N, H, W, C1, C2, Hs, Ws, da, acc_a);
-    upcat_bwd_skip_kernel<<<grid_n((size_t)N * H * W * C2), 256, 0, st>>>(dout, (size_t)N * H * W, C1, C2, dskip,
+    upcat_bwd_a_kernel<<<grid_n((size_t)N * Hs * Ws * C1 / 8), 256, 0, st>>>(dout, N, H, W, C1, C2, Hs, Ws, da, acc_a);
+    upcat_bwd_skip_kernel<<<grid_n((size_t)N * H * W * C2 / 8), 256, 0, st>>>(dout, (size_t)N * H * W, C1, C2, dskip,
                                                                          acc_skip);
 }
 
 void nn_relu_bwd(const float* da, const void* a, size_t n, void* dpre, cudaStream_t st) {
-    relu_bwd_kernel<<<grid_n(n), 256, 0, st>>>(da, static_cast<const __nv_bfloat16*>(a), n,
+    relu_bwd_kernel<<<grid_n(n / 8), 256, 0, st>>>(da, static_cast<const __nv_bfloat16*>(a), n,
                                                static_cast<__nv_bfloat16*>(dpre));
 }
 

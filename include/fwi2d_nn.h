@@ -9,7 +9,9 @@
  *   - activation gradients, master weights, optimiser state: float32;
  *   - weights: [Cout][3][3][Cin], biases: [Cout];
  *   - every call enqueues on `stream` (a cudaStream_t, NULL = default) and
- *     returns 0, or FWI_ERR_ARG for unsupported sizes.
+ *     returns 0, or FWI_ERR_ARG for unsupported sizes;
+ *   - buffers start on 16-byte boundaries and channel counts (and relu_bwd's
+ *     n) are multiples of 8: the kernels move 8 channels at a time.
  * The 3x3 convolutions (zero padding) are implicit GEMMs on the BF16 tensor
  * cores with FP32 accumulation.
  */
