@@ -126,8 +126,9 @@ struct ConvArgs {
     int H, W, Cout;
     int bw, tiles_x, tiles_y, ntiles;
     int cb, nkb, sw;  // channels per block, blocks per tap, row bytes (= 2 cb)
+    int bps;          // channel blocks per stage (> 1: one 5-D input box and one 4-D weight box per stage)
     int stages;
-    uint32_t stage_bytes, a_bytes, tx_bytes;
+    uint32_t stage_bytes, a_bytes, tx_bytes;  // a_bytes: the stage's input boxes
     int ncols;  // TMEM columns allocated (>= 2 Cout)
     const float* bias;
     int relu;
@@ -173,7 +174,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     fence_after();
     const uint32_t tmem = tmem_slot;
-    const int nk = 9 * a.nkb;  // stages per tile
+    const int spt = a.nkb / a.bps;  // stages per tap
+    const int nk = 9 * spt;         // stages per tile
     bool ok = true;
 
     if (warp == 0) {
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 int n, x0, y0;
                 conv_tile_origin(a, t, n, x0, y0);
                 for (int kk = 0; kk < nk; ++kk, ++it) {
-                    const int tap = kk / a.nkb, kb = kk - tap * a.nkb;
+                    const int tap = kk / spt, kb = (kk - tap * spt) * a.bps;  // first channel block of the stage
                     const int s = (int)(it % (uint32_t)a.stages);
                     const uint32_t use = it / (uint32_t)a.stages;
                     if (!tma::mbar_wait(&empty[s], (use & 1u) ^ 1u)) {
@@ -192,8 +194,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     unsigned char* A = smem + (size_t)s * a.stage_bytes;
                     tma::mbar_arrive_expect_tx(&full[s], a.tx_bytes);
-                    tma::load_4d(A, &m_in, kb * a.cb, x0 + tap % 3 - 1, y0 + tap / 3 - 1, n, &full[s]);
-                    tma::load_3d(A + a.a_bytes, &m_w, kb * a.cb, tap, 0, &full[s]);
+                    if (a.bps == 1) {
+                        tma::load_4d(A, &m_in, kb * a.cb, x0 + tap % 3 - 1, y0 + tap / 3 - 1, n, &full[s]);
+                        tma::load_3d(A + a.a_bytes, &m_w, kb * a.cb, tap, 0, &full[s]);
+                    } else {
+                        // (channel, x, y, image, block) and (channel, co, tap, block): bps blocks back to back
+                        tma::load_5d(A, &m_in, 0, x0 + tap % 3 - 1, y0 + tap / 3 - 1, n, kb, &full[s]);
+                        tma::load_4d(A + a.a_bytes, &m_w, 0, 0, tap, kb, &full[s]);
+                    }
                 }
             }
             // the last fill of every stage has landed before the CTA can exit
@@ -223,9 +231,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     fence_after();
                     const uint32_t sa = saddr(smem + (size_t)s * a.stage_bytes), sb = sa + a.a_bytes;
-                    for (int k = 0; k < a.cb / 16; ++k)
-                        mma(d, mdesc(sa + 32u * k, 16u, sbo, lay), mdesc(sb + 32u * k, 16u, sbo, lay), id,
-                            (kk | k) != 0);
+                    for (int b = 0; b < a.bps; ++b) {
+                        const uint32_t ab = sa + (uint32_t)b * kConvM * a.sw, bb = sb + (uint32_t)(b * a.Cout * a.sw);
+                        for (int k = 0; k < a.cb / 16; ++k)
+                            mma(d, mdesc(ab + 32u * k, 16u, sbo, lay), mdesc(bb + 32u * k, 16u, sbo, lay), id,
+                                (kk | b | k) != 0);
+                    }
                     commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -700,6 +711,34 @@ bool weight_map(CUtensorMap* m, const void* base, int Cin, int Cout, int cb) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The input as (cb, W, H, N, C / cb): the channel blocks of a pixel as a fifth
+// dimension (stride 2 cb bytes), box (cb, bw, bh, 1, bps) = bps blocks of
+// 128 pixel rows back to back.
+bool act_blocks_map(CUtensorMap* m, const void* base, int N, int H, int W, int C, int cb, int bw, int bh, int bps) {
+    auto enc = encoder();
+    if (!enc) return false;
+    cuuint64_t dims[5] = {(cuuint64_t)cb, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N, (cuuint64_t)(C / cb)};
+    cuuint64_t strides[4] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2, (cuuint64_t)cb * 2};
+    cuuint32_t box[5] = {(cuuint32_t)cb, (cuuint32_t)bw, (cuuint32_t)bh, 1, (cuuint32_t)bps};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(2 * cb), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Weights [Cout][9][Cin] as (cb, Cout, 9, Cin / cb), box (cb, Cout, 1, bps).
+bool weight_blocks_map(CUtensorMap* m, const void* base, int Cin, int Cout, int cb, int bps) {
+    auto enc = encoder();
+    if (!enc) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)cb, (cuuint64_t)Cout, 9, (cuuint64_t)(Cin / cb)};
+    cuuint64_t strides[3] = {(cuuint64_t)Cin * 9 * 2, (cuuint64_t)Cin * 2, (cuuint64_t)cb * 2};
+    cuuint32_t box[4] = {(cuuint32_t)cb, (cuuint32_t)Cout, 1, (cuuint32_t)bps};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(2 * cb), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Width of a box of `pixels` pixels (width x height = pixels, both powers of
 // two, height <= 32) that pads the H x W image least; ties go to the wider box.
 int box_width(int H, int W, int pixels) {
@@ -869,8 +908,18 @@ int nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, 
     a.cb = channel_block(Cin);
     a.nkb = Cin / a.cb;
     a.sw = 2 * a.cb;
-    a.a_bytes = (uint32_t)kConvM * a.sw;
-    const uint32_t b_bytes = (uint32_t)Cout * a.sw;
+    // 128-byte rows: as many channel blocks per stage as divide the tap's and
+    // keep the stage within kStageCap (each block's weights Cout x 128 B, a
+    // multiple of the 1024-B swizzle span)
+    a.bps = 1;
+    if (a.cb == 64)
+        for (int b = a.nkb; b > 1; --b)
+            if (a.nkb % b == 0 && (uint32_t)b * (kConvM + Cout) * 128u <= kStageCap) {
+                a.bps = b;
+                break;
+            }
+    a.a_bytes = (uint32_t)a.bps * kConvM * a.sw;
+    const uint32_t b_bytes = (uint32_t)(a.bps * Cout * a.sw);
     a.tx_bytes = a.a_bytes + b_bytes;
     a.stage_bytes = (a.tx_bytes + 1023u) / 1024u * 1024u;
     size_t stages = (cap - 1024) / a.stage_bytes;
@@ -883,7 +932,13 @@ int nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, 
     a.out = static_cast<__nv_bfloat16*>(out);
     a.out32 = out32;
     CUtensorMap mi, mw;
-    if (!act_map(&mi, in, N, H, W, Cin, a.cb, a.bw, bh) || !weight_map(&mw, w, Cin, Cout, a.cb)) return -2;
+    if (a.bps > 1) {
+        if (!act_blocks_map(&mi, in, N, H, W, Cin, a.cb, a.bw, bh, a.bps) ||
+            !weight_blocks_map(&mw, w, Cin, Cout, a.cb, a.bps))
+            return -2;
+    } else if (!act_map(&mi, in, N, H, W, Cin, a.cb, a.bw, bh) || !weight_map(&mw, w, Cin, Cout, a.cb)) {
+        return -2;
+    }
     size_t dyn = (size_t)a.stages * a.stage_bytes + 1024;
     if (dyn < kOneCtaPerSm) dyn = kOneCtaPerSm;
     const int grid = a.ntiles < sm_count() ? a.ntiles : sm_count();

@@ -87,5 +87,15 @@ __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* m, int c0,
         : "memory");
 }
 
+// 5-D tiled load of box (c0, c1, c2, c3, c4); c0 as for load_4d.
+__device__ __forceinline__ void load_5d(void* dst, const CUtensorMap* m, int c0, int c1, int c2, int c3, int c4,
+                                        uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+        : "memory");
+}
+
 }  // namespace tma
 }  // namespace fwi
