@@ -244,6 +244,8 @@ def profile_case(which: str = "large"):
         torch.cuda.synchronize()
         print("profile case done: unet", float(net.loss.item()))
         return
+    if which == "unet-time":
+        return unet_timing()
     if which == "batched":
         # 60 of the 240 windowed shots (every 4th), nt 40: one RTM = one
         # forward and one backward multi-level launch, fields ~1.9 GB > L2
@@ -264,6 +266,78 @@ def profile_case(which: str = "large"):
     with api.Context(case.params, api.MODE_MODELING) as ctx:
         ctx.model_survey_raw()
         print("profile case done:", ctx.describe())
+
+
+def unet_timing(reps: int = 20) -> None:
+    """CUDA-event timing of the CNN preconditioner's kernels: one forward + MSE
+    + backward pass on a 1701 x 301 image (the FWI model), one training step
+    (pass + Adam) on 4 images of 501 x 151 (the training models), and each
+    layer's forward, data-gradient and weight-gradient convolution alone.
+    Prints one JSON line."""
+    import torch
+
+    from fwi2d_b200 import api, cnn
+    L = api.lib()
+
+    def timed(fn, n=reps):
+        for _ in range(3):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n * 1e3  # us
+
+    def image(N, H, W):
+        x = torch.zeros(N * H * W * cnn.IN_CH, dtype=torch.bfloat16, device="cuda")
+        x.view(-1, cnn.IN_CH)[:, :3] = torch.randn(N * H * W, 3, device="cuda").to(torch.bfloat16)
+        return x, torch.randn(N * H * W, device="cuda")
+
+    out = {}
+    for key, (N, H, W, adam) in {"pass_1701x301_us": (1, 1701, 301, False),
+                                 "train_step_4x501x151_us": (4, 501, 151, True)}.items():
+        net = cnn.UNet(seed=0)
+        x, t = image(N, H, W)
+
+        def step():
+            net.forward(x, N, H, W)
+            net.mse(t)
+            net.backward(x, net.dout)
+            if adam:
+                net.adam()
+        out[key] = round(timed(step), 1)
+    net = cnn.UNet(seed=0)
+    N, H, W = 1, 1701, 301
+    x, t = image(N, H, W)
+    net.forward(x, N, H, W)
+    layers = {}
+    for c in net.layers:
+        h, w = net.dims[net.level[c.name]]
+        src = net._input_of(c.name, x)
+        y = torch.empty(N * h * w * c.cout, dtype=torch.bfloat16, device="cuda")
+        gx = torch.empty(N * h * w * c.cin, dtype=torch.float32, device="cuda")
+        dy = torch.randn(N * h * w * c.cout, device="cuda").to(torch.bfloat16)
+        flop = 2.0 * N * h * w * 9 * c.cin * c.cout
+        calls = {
+            "fwd": lambda: L.fwi_nn_conv3x3(src.data_ptr(), N, h, w, c.cin, c.w16.data_ptr(), c.b.data_ptr(), c.cout,
+                                            1, y.data_ptr(), None, None),
+            "dgrad": lambda: L.fwi_nn_conv3x3(dy.data_ptr(), N, h, w, c.cout, c.wt16.data_ptr(), None, c.cin, 0, None,
+                                              gx.data_ptr(), None),
+            "wgrad": lambda: L.fwi_nn_conv3x3_wgrad(src.data_ptr(), dy.data_ptr(), N, h, w, c.cin, c.cout,
+                                                    net.partial.data_ptr(), c.gw.data_ptr(), c.gb.data_ptr(), None),
+        }
+        row = {"size": f"{h}x{w}", "cin": c.cin, "cout": c.cout}
+        for kind, fn in calls.items():
+            us = timed(fn)
+            row[kind + "_us"] = round(us, 1)
+            row[kind + "_tflops"] = round(flop / us / 1e6, 1)
+        layers[c.name] = row
+    out["layers"] = layers
+    if L.fwi_nn_check() != 0:
+        raise RuntimeError("a bounded wait of the tensor-core kernels gave up")
+    print(json.dumps(out))
 
 
 def batched_survey(peak: float, nt: int = 300, reps: int = 2) -> dict:
@@ -499,9 +573,11 @@ def main():
                     help="FWI iterations of the 81-shot survey companion measurement (0: skip)")
     ap.add_argument("--fwi-batched-iterations", type=int, default=1,
                     help="FWI iterations of the 240-shot windowed survey companion measurement (0: skip)")
-    ap.add_argument("--profile", nargs="?", const="large", choices=["large", "small", "batched", "unet", "resident"],
+    ap.add_argument("--profile", nargs="?", const="large",
+                    choices=["large", "small", "batched", "unet", "resident", "unet-time"],
                     help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
-                         "time axis; small: the benchmark survey)")
+                         "time axis; small: the benchmark survey); unet: the CNN's forward + backward; unet-time: "
+                         "CUDA-event timing of the CNN's kernels (no ncu)")
     args = ap.parse_args()
     if args.profile:
         return profile_case(args.profile)
