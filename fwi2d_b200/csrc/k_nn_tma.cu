@@ -212,6 +212,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             const uint32_t id = idesc(kConvM, a.Cout, false, false);
             const uint32_t lay = layout_of(a.sw), sbo = 8u * (uint32_t)a.sw;
+            // the A and B descriptors of stage 0, block 0; others are constant offsets
+            const uint64_t d0 = mdesc(saddr(smem), 16u, sbo, lay);
+            const uint64_t blk_a = ((uint64_t)kConvM * a.sw) >> 4, blk_b = ((uint64_t)a.Cout * a.sw) >> 4;
             uint32_t it = 0;
             int local = 0;
             for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++local) {
@@ -230,13 +233,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     fence_after();
-                    const uint32_t sa = saddr(smem + (size_t)s * a.stage_bytes), sb = sa + a.a_bytes;
-                    for (int b = 0; b < a.bps; ++b) {
-                        const uint32_t ab = sa + (uint32_t)b * kConvM * a.sw, bb = sb + (uint32_t)(b * a.Cout * a.sw);
-                        for (int k = 0; k < a.cb / 16; ++k)
-                            mma(d, mdesc(ab + 32u * k, 16u, sbo, lay), mdesc(bb + 32u * k, 16u, sbo, lay), id,
-                                (kk | b | k) != 0);
-                    }
+                    const uint64_t da = d0 + (uint64_t)s * (a.stage_bytes >> 4), db = da + (a.a_bytes >> 4);
+                    for (int b = 0; b < a.bps; ++b)
+                        for (int k = 0; k < a.cb / 16; ++k)  // K step: 32 B along the swizzled row
+                            mma(d, da + b * blk_a + 2 * k, db + b * blk_b + 2 * k, id, (kk | b | k) != 0);
                     commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -391,10 +391,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             const uint32_t id_b = idesc(128, 16, true, true);
+            // one MMA per group of tps taps (N = tps x Cin); the last group may be shorter
+            const uint32_t id_full = idesc(128, a.tps * a.Cin, true, true);
+            const uint32_t id_tail = idesc(128, (ntap - (ntap - 1) / a.tps * a.tps) * a.Cin, true, true);
             const uint32_t la = layout_of(a.swo), lb = layout_of(a.swi);
             const uint32_t sbo_a = 8u * (uint32_t)a.swo, sbo_b = 8u * (uint32_t)a.swi;
             const uint32_t lbo_b = (uint32_t)kWgK * (uint32_t)a.swi;
             const uint64_t d_ones = mdesc(saddr(ones), 128u, 256u, 0u);
+            // stage 0's descriptors; a stage, K step and tap group are constant offsets
+            const uint64_t da0 = mdesc(saddr(smem), a.a_lbo, sbo_a, la);
+            const uint64_t db0 = mdesc(saddr(smem) + a.a_bytes, lbo_b, sbo_b, lb);
+            const uint64_t k_a = (16u * (uint32_t)a.swo) >> 4, k_b = (16u * (uint32_t)a.swi) >> 4;
+            const uint64_t grp_b = ((uint64_t)a.tps * a.b_bytes) >> 4;
             uint32_t it = 0;
             for (int t = t_begin; t < t_end; ++t, ++it) {
                 const int s = (int)(it % (uint32_t)a.stages);
@@ -403,20 +411,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 fence_after();
-                const uint32_t sa = saddr(smem + (size_t)s * a.stage_bytes), sb = sa + a.a_bytes;
+                const uint64_t ds = (uint64_t)s * (a.stage_bytes >> 4);
                 for (int k = 0; k < kWgK / 16; ++k) {
                     // K step: 16 pixels = two 8-row groups of each operand
-                    const uint64_t da = mdesc(sa + 16u * k * (uint32_t)a.swo, a.a_lbo, sbo_a, la);
+                    const uint64_t da = da0 + ds + k * k_a;
                     const bool acc = (it | (uint32_t)k) != 0;
                     // the taps' input blocks are b_bytes = nbi x kWgK x swi apart, i.e. every
                     // cbi-channel block of the group sits lbo_b after the previous one: up to tps
                     // taps form one MMA with N = taps x Cin
-                    for (int j = 0; j < ntap; j += a.tps) {
-                        const int nt = ntap - j < a.tps ? ntap - j : a.tps;
-                        mma(tmem + (uint32_t)(j * a.Cin), da,
-                            mdesc(sb + (uint32_t)j * a.b_bytes + 16u * k * (uint32_t)a.swi, lbo_b, sbo_b, lb),
-                            idesc(128, nt * a.Cin, true, true), acc);
-                    }
+                    for (int j = 0, g = 0; j < ntap; j += a.tps, ++g)
+                        mma(tmem + (uint32_t)(j * a.Cin), da, db0 + ds + g * grp_b + k * k_b,
+                            ntap - j < a.tps ? id_tail : id_full, acc);
                     if (with_bias) mma(tmem + (uint32_t)(ntap * a.Cin), da, d_ones, id_b, acc);
                 }
                 commit(&empty[s]);
@@ -570,7 +575,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             const uint32_t id = idesc(kConvM, a.Cout, false, false);
-            const uint32_t wb = saddr(smem), wstep = (uint32_t)a.Cout * 16u;
+            // descriptors built once: one thread's dependent integer chain per
+            // descriptor costs more than the MMA it feeds, so a tap's operands are
+            // a base plus constant offsets (16-byte units)
+            const uint32_t wstep = (uint32_t)a.Cout * 16u;
+            const uint64_t dw0 = mdesc(saddr(smem), wstep, 128u, 0u);
+            const uint64_t dh0 = mdesc(saddr(ring), kHaloPlane, kHaloRow, 0u);
+            const uint64_t tap_w = ((uint64_t)kc * wstep) >> 4, k_w = (2u * wstep) >> 4, k_h = (2u * kHaloPlane) >> 4;
             int s = 0, local = 0;
             uint32_t ph = 0;
             for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++local) {
@@ -582,14 +593,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 fence_after();
                 const uint32_t d = tmem + (uint32_t)(acc * a.Cout);
-                const uint32_t hb = saddr(ring + (size_t)s * a.stage_bytes);
+                const uint64_t dh = dh0 + (uint64_t)s * (a.stage_bytes >> 4);
+#pragma unroll
                 for (int tap = 0; tap < 9; ++tap) {
-                    const uint64_t da0 = mdesc(hb + tap_offset(tap), kHaloPlane, kHaloRow, 0u);
-                    const uint64_t db0 = mdesc(wb + (uint32_t)(tap * kc) * wstep, wstep, 128u, 0u);
-                    for (int k = 0; k < kc / 2; ++k)
-                        // K step k: planes 2k, 2k + 1 (start addresses advance in 16-B units)
-                        mma(d, da0 + (uint64_t)((2u * k * kHaloPlane) >> 4), db0 + (uint64_t)((2u * k * wstep) >> 4),
-                            id, (tap | k) != 0);
+                    const uint64_t da = dh + (tap_offset(tap) >> 4), db = dw0 + (uint64_t)tap * tap_w;
+                    mma(d, da, db, id, tap != 0);
+                    // K steps 1..: planes 2k, 2k + 1
+                    for (int k = 1; k < kc / 2; ++k) mma(d, da + k * k_h, db + k * k_w, id, true);
                 }
                 commit(&empty[s]);
                 commit(&tfull[acc]);
