@@ -784,17 +784,23 @@ int sm_count() {
     return n;
 }
 
-// Largest dynamic shared memory the kernel may take (set on first use).
+// Largest dynamic shared memory the kernel may take, set for the current
+// device on its first use there (function attributes are per device).
+constexpr int kMaxDevices = 64;
+
 template <typename K>
-size_t max_dynamic_smem(K kernel) {
+size_t max_dynamic_smem(K kernel, size_t (&per_device)[kMaxDevices]) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    if (per_device[dev] != 0) return per_device[dev];
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
     const size_t cap = 227 * 1024 - fa.sharedSizeBytes;
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) != cudaSuccess) return 0;
-    return cap;
+    return per_device[dev] = cap;
 }
 
-constexpr uint32_t kStageCap = 72 * 1024;  // weight-gradient stage bound
+constexpr uint32_t kStageCap = 72 * 1024;  // bound of a weight-gradient stage and of a convolution stage of several channel blocks
 
 struct WgPlan {
     WgradArgs a;
@@ -885,8 +891,9 @@ int nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, 
                    void* out, float* out32, cudaStream_t st) {
     if (Cin % 16 || Cin > 256 || Cout % 16 || Cout > 256 || N < 1 || H < 1 || W < 1) return -1;
     if (!aligned16(in) || !aligned16(w) || !aligned16(out) || !aligned16(out32)) return -1;
-    static size_t hcap = 0;
-    if (hcap == 0 && (hcap = max_dynamic_smem(conv3x3_halo_kernel)) == 0) return -2;
+    static size_t hcaps[kMaxDevices] = {};
+    const size_t hcap = max_dynamic_smem(conv3x3_halo_kernel, hcaps);
+    if (hcap == 0) return -2;
     HaloConvArgs h;
     if (halo_conv_plan(N, H, W, Cin, Cout, hcap, h)) {
         h.w = static_cast<const __nv_bfloat16*>(w);
@@ -902,8 +909,9 @@ int nn_conv3x3_tma(const void* in, int N, int H, int W, int Cin, const void* w, 
         conv3x3_halo_kernel<<<grid, kThreads, dyn, st>>>(mh, h);
         return cudaGetLastError() == cudaSuccess ? 0 : -2;
     }
-    static size_t cap = 0;
-    if (cap == 0 && (cap = max_dynamic_smem(conv3x3_tma_kernel)) == 0) return -2;
+    static size_t caps[kMaxDevices] = {};
+    const size_t cap = max_dynamic_smem(conv3x3_tma_kernel, caps);
+    if (cap == 0) return -2;
     ConvArgs a{};
     a.H = H;
     a.W = W;
@@ -965,8 +973,9 @@ size_t nn_wgrad_tma_partial_floats(int N, int H, int W, int Cin, int Cout) {
 int nn_wgrad_tma(const void* in, const void* dout, int N, int H, int W, int Cin, int Cout, float* partial, bool bias,
                  cudaStream_t st) {
     if (!aligned16(in) || !aligned16(dout) || !aligned16(partial)) return -1;
-    static size_t cap = 0;
-    if (cap == 0 && (cap = max_dynamic_smem(wgrad_tma_kernel)) == 0) return -2;
+    static size_t caps[kMaxDevices] = {};
+    const size_t cap = max_dynamic_smem(wgrad_tma_kernel, caps);
+    if (cap == 0) return -2;
     WgPlan p;
     if (!wg_plan(N, H, W, Cin, Cout, cap, p)) return -1;
     WgradArgs a = p.a;

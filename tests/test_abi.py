@@ -47,3 +47,24 @@ def test_create_failure_reports_error_without_gpu(tmp_path):
         assert e.code == -2 and "could not be opened" in str(e)
     else:
         raise AssertionError("expected FwiError")
+
+
+def test_nn_kernels_refuse_unsupported_sizes_without_gpu():
+    """The CNN entry points check sizes and alignment before any CUDA call:
+    channel counts that are not multiples of 8 (16 for the convolutions),
+    buffers off a 16-byte boundary and ReLU-gradient lengths that are not
+    multiples of 8 return FWI_ERR_ARG (-8)."""
+    L = api.lib()
+    ok, odd = 1 << 20, (1 << 20) + 8  # addresses only compared, never read
+    assert L.fwi_nn_pool2(ok, 1, 4, 4, 12, ok, None) == -8
+    assert L.fwi_nn_pool2(odd, 1, 4, 4, 16, ok, None) == -8
+    assert L.fwi_nn_pool2_bwd(ok, 1, 4, 4, 20, ok, 0, None) == -8
+    assert L.fwi_nn_upcat(ok, 2, 2, 12, ok, 1, 4, 4, 16, ok, None) == -8
+    assert L.fwi_nn_upcat(ok, 2, 2, 16, ok, 1, 4, 4, 16, odd, None) == -8
+    assert L.fwi_nn_upcat_bwd(ok, 1, 4, 4, 16, 4, 2, 2, ok, 0, ok, 0, None) == -8
+    assert L.fwi_nn_relu_bwd(ok, ok, 100, ok, None) == -8
+    assert L.fwi_nn_relu_bwd(ok, odd, 128, ok, None) == -8
+    assert L.fwi_nn_mse(ok, 12, ok, None, 16, 1.0, ok, ok, ok, None) == -8
+    assert L.fwi_nn_conv3x3(ok, 1, 8, 8, 24, ok, None, 16, 0, ok, None, None) == -8
+    assert L.fwi_nn_conv3x3(odd, 1, 8, 8, 16, ok, None, 16, 0, ok, None, None) == -8
+    assert L.fwi_nn_conv3x3(ok, 1, 8, 8, 16, ok, None, 272, 0, ok, None, None) == -8
