@@ -183,11 +183,22 @@ __global__ void __launch_bounds__(32 * kWarps) wgrad_kernel(const __nv_bfloat16*
 // eight slices are then added in slice order.  nw is a multiple of 4.
 constexpr int kSlices = 8;
 
+// Blocks past nblocks_w reduce a second array (nb values after the first's
+// chunks x nw partials, e.g. the bias partials) into db in the same way.
 __global__ void __launch_bounds__(32 * kSlices) wgrad_reduce_kernel(const float* __restrict__ partial, int chunks,
-                                                                    size_t nw, float* __restrict__ dw) {
+                                                                    size_t nw, float* __restrict__ dw,
+                                                                    unsigned nblocks_w = 0, size_t nb = 0,
+                                                                    float* __restrict__ db = nullptr) {
     __shared__ float4 red[kSlices][32];
+    unsigned blk = blockIdx.x;
+    if (db && blk >= nblocks_w) {  // the second array
+        partial += (size_t)chunks * nw;
+        nw = nb;
+        dw = db;
+        blk -= nblocks_w;
+    }
     const int col = threadIdx.x & 31, slice = threadIdx.x >> 5;
-    const size_t i = ((size_t)blockIdx.x * 32 + col) * 4;
+    const size_t i = ((size_t)blk * 32 + col) * 4;
     float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (i < nw) {
 #pragma unroll 4
@@ -572,10 +583,9 @@ int nn_conv3x3_wgrad(const void* in, const void* dout, int N, int H, int W, int 
         const int tc_chunks = nn_wgrad_tma(in, dout, N, H, W, Cin, Cout, partial, db != nullptr, st);
         if (tc_chunks == -2) return -2;
         if (tc_chunks > 0) {
-            wgrad_reduce_kernel<<<reduce_blocks(nw), 32 * kSlices, 0, st>>>(partial, tc_chunks, nw, dw);
-            if (db)
-                wgrad_reduce_kernel<<<reduce_blocks((size_t)Cout), 32 * kSlices, 0, st>>>(partial + (size_t)tc_chunks * nw, tc_chunks,
-                                                                          (size_t)Cout, db);
+            // the weight partials, then (db) the bias partials stored after them, in one launch
+            const unsigned bw = reduce_blocks(nw), bb = db ? reduce_blocks((size_t)Cout) : 0u;
+            wgrad_reduce_kernel<<<bw + bb, 32 * kSlices, 0, st>>>(partial, tc_chunks, nw, dw, bw, (size_t)Cout, db);
             return 0;
         }
     }
