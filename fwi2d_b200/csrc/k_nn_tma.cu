@@ -5,8 +5,9 @@
 // tensor memory) and the commits, warps 2-5 read the accumulators back with
 // `tcgen05.ld.32x32b` (each its 32-lane quarter).  CTAs are persistent, one
 // per SM.  Every fixed cost here is per instruction of one thread (about
-// 60 ns a TMA load, 30 ns an MMA on this part), so the kernels are shaped to
-// issue few, wide operations per pixel.
+// 60 ns a TMA load, 35-50 ns an MMA on this part, plus the thread's own
+// integer work: descriptors are built once and offset by constants), so the
+// kernels are shaped to issue few, wide operations per pixel.
 //
 // Convolution D[p, co] = sum_{tap, ci} in[p + tap, ci] w[co, tap, ci], two kernels:
 //   * conv3x3_halo_kernel (the weights fit in shared memory next to the
