@@ -246,6 +246,19 @@ def profile_case(which: str = "large"):
         return
     if which == "unet-time":
         return unet_timing()
+    if which == "batch-sweep":
+        # RTM of the 240-shot survey with 240, 120 and 80 shots per batch
+        peak, _ = peaks()
+        out = {}
+        for bs in (240, 120, 80):
+            for nt in (300, 4001):
+                r = batched_survey(peak, nt=nt, reps=2 if nt == 300 else 1, batch_shots=bs)
+                out[f"{bs}_shots_nt{nt}"] = {
+                    "forward_frac": r["forward"]["frac"], "backward_frac": r["backward"]["frac"],
+                    "rtm_s": (r["forward"]["ms"] + r["backward"]["ms"]) / (2 if nt == 300 else 1) / 1e3,
+                    "launches": r["forward"]["launches"], "peak_gbs": peak}
+        print(json.dumps(out))
+        return
     if which == "batched":
         # 60 of the 240 windowed shots (every 4th), nt 40: one RTM = one
         # forward and one backward multi-level launch, fields ~1.9 GB > L2
@@ -340,14 +353,16 @@ def unet_timing(reps: int = 20) -> None:
     print(json.dumps(out))
 
 
-def batched_survey(peak: float, nt: int = 300, reps: int = 2) -> dict:
+def batched_survey(peak: float, nt: int = 300, reps: int = 2, batch_shots: int | None = None) -> dict:
     """HBM-bound companion measurement: the batched uneven-aperture survey
-    (240 shots of the 301x1701 FWI model, each on its own window, all in one
-    batch), RTM through the random boundary with nt time samples; forward and
-    backward kernels timed by CUDA events on the engine stream."""
+    (240 shots of the 301x1701 FWI model, each on its own window; the engine's
+    default batches, or batch_shots per batch), RTM through the random boundary
+    with nt time samples; forward and backward kernels timed by CUDA events on
+    the engine stream."""
     from fwi2d_b200 import api, synth
     d = Path(tempfile.mkdtemp(prefix="fwi2d_batched_"))
-    case, _ = synth.aperture_survey(d, nt=nt)
+    extra = {"batch_shots": batch_shots} if batch_shots else {}
+    case, _ = synth.aperture_survey(d, nt=nt, **extra)
     with api.Context(case.params, api.MODE_MIGRATION) as ctx:
         dims = ctx.dims
         widths = [ctx.window(s)[1] for s in range(dims.nsrc)]
@@ -574,10 +589,11 @@ def main():
     ap.add_argument("--fwi-batched-iterations", type=int, default=1,
                     help="FWI iterations of the 240-shot windowed survey companion measurement (0: skip)")
     ap.add_argument("--profile", nargs="?", const="large",
-                    choices=["large", "small", "batched", "unet", "resident", "unet-time"],
+                    choices=["large", "small", "batched", "unet", "resident", "unet-time", "batch-sweep"],
                     help="for ncu: one forward survey (large: 81 shots on 501x1901, fields ~630 MB > L2, short "
                          "time axis; small: the benchmark survey); unet: the CNN's forward + backward; unet-time: "
-                         "CUDA-event timing of the CNN's kernels (no ncu)")
+                         "CUDA-event timing of the CNN's kernels; batch-sweep: RTM of the 240-shot survey in "
+                         "batches of 240, 120 and 80 shots (both no ncu)")
     args = ap.parse_args()
     if args.profile:
         return profile_case(args.profile)
