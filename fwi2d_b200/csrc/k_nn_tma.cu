@@ -17,7 +17,9 @@
 //     weights stay resident for the CTA's life;
 //   * conv3x3_tma_kernel (large weights): a tile is a bw x bh box of 128
 //     pixels; per (tap, channel block of 64 / 32 / 16) one swizzled 4-D box of
-//     the shifted pixels (zero fill gives the padding) and one of the weights.
+//     the shifted pixels (zero fill gives the padding) and one of the weights,
+//     or, with 64-channel blocks, one 5-D box of several blocks and one 4-D
+//     box of their weights per stage.
 //   Both keep two TMEM accumulators (M = 128 lanes x Cout columns) so the
 //   epilogue of a tile (bias, ReLU, NHWC store) overlaps the next tile's MMAs.
 //
